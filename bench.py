@@ -1,0 +1,349 @@
+"""Benchmark: DOF-stage updates/s of the SDDC drop-in on one or more B200s.
+
+Workload: the cylinder case on the 256 radial x 512 circumferential O-grid
+with p = 4 (N = 5; 131,072 cells, 3,276,800 solution points x 9 variables),
+RK_S5P3 at CFL 0.3.  One step = one RK3 step = 5 fused stage launches over
+every cell.  The state registers (236 MB each) are larger than the 126 MB L2,
+so no flush is needed between steps.
+
+Arms:
+* default (ours): the mixed form is the headline ``value``; the FP64 and the
+  FP64-exact forms are timed on the same workload beside it.  ``e2e`` runs the
+  same steps through the C ABI with host buffers (state in, step, state and
+  monitor out, every step).  ``cpu_baseline`` times the CPU oracle (the
+  restatement of the reference's FP64 path) on the host cores.
+* ``--impl reference``: the reference's own path on the CPU, i.e. the oracle
+  restatement (the Fortran reference cannot be built here), all host cores.
+
+Multi-GPU (torchrun): every rank runs an independent replica of the
+workload (the drop-in is single-GPU; the case does not shard), timing is the
+max over ranks and ``value`` is the total over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "DOF-stage updates/s (mixed vs FP64, same B200, rel-L2≤1e-6); adjoint cost ratio"
+UNIT = "DOF-stage updates/s"
+NR, NT, NPTS = 256, 512, 5
+MS, MA = 0.5, 2.0  # Ms = 1.5 diverges within ~10 steps in the reference algorithm (AV off)
+
+
+def bytes_per_dof_stage(N: int) -> float:
+    """Algorithmic HBM bytes per DOF-stage: 3*9*8 (state in, state out, RK
+    register traffic averaged over RK_S5P3) + 8 (Jac) + 32(N+1)/N (the four
+    metric normals at the 2N(N+1) flux points)."""
+    return 3 * 9 * 8 + 8 + 32.0 * (N + 1) / N
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_case():
+    from sddc_b200 import cases, host
+
+    c = cases.cylinder_case(NR, NT, NPTS, ms=MS, ma=MA, seed=0, noise=1e-6)
+    t = host.build_tables(c.mesh, c.N)
+    Q0 = c.initial_state(t)
+    dt = cases.cfl_dt(c.mesh, Q0, c.N, 0.3)
+    return c, t, Q0, dt
+
+
+class Clocks:
+    """nvidia-smi clock samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def time_form(torch, solver_mod, t, ph, Q0, dt, precision, steps, warmup):
+    """Device time of `steps` RK3 steps (state resident), CUDA events on the
+    context's stream."""
+    s = solver_mod.Solver(t, ph, precision=precision)
+    s.set_state(Q0)
+    s.rk_s5p3(dt, warmup)
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.rk_s5p3(dt, steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    return s, ms
+
+
+def run_ours(args):
+    import torch
+
+    from sddc_b200 import solver as solver_mod
+
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    c, t, Q0, dt = build_case()
+    ph = c.physics
+    dof = c.mesh.ncell * c.N * c.N
+    steps, warm = args.steps, args.warmup
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    results = {}
+    states = {}
+    try:
+        gpu_index = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_index = str(local)
+    clocks = None
+    for prec in ("mixed", "fp64", "fp64_exact"):
+        barrier()
+        if prec == "mixed":
+            with Clocks(gpu_index) as ck:
+                s, ms = time_form(torch, solver_mod, t, ph, Q0, dt, prec, steps, warm)
+            clocks = ck.summary()
+        else:
+            s, ms = time_form(torch, solver_mod, t, ph, Q0, dt, prec, steps, warm)
+        if dist:
+            m = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+            ms = float(m.item())
+        results[prec] = ms
+        states[prec] = s.state()["Q"]
+        s.close()
+    barrier()
+    # end-to-end through the C ABI with host buffers, every step:
+    # state host->device, one RK3 step, state and monitor device->host
+    s = solver_mod.Solver(t, ph, precision="mixed")
+    q_host = torch.empty(Q0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(Q0.shape, order="F")
+    q_host[...] = Q0
+    out_host = torch.empty(Q0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(Q0.shape, order="F")
+    s.set_state(q_host)
+    s.rk_s5p3(dt, 1)
+    e2e_steps = max(3, min(steps, 20))
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s.set_state(q_host)
+        s.rk_s5p3(dt, 1)
+        s.state(out=out_host)
+        s.monitor()
+        q_host, out_host = out_host, q_host
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    s.close()
+    if dist:
+        m = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        e2e_ms = float(m.item())
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    ref = states["fp64_exact"]
+    acc = {
+        "mixed_vs_fp64_exact_rel_l2": float(np.linalg.norm(states["mixed"] - ref) / np.linalg.norm(ref)),
+        "fp64_vs_fp64_exact_rel_l2": float(np.linalg.norm(states["fp64"] - ref) / np.linalg.norm(ref)),
+        "after_steps": steps + warm,
+        "note": "fp64_exact is bit-equal to the CPU oracle (tests/test_gpu_parity.py)",
+    }
+    units = dof * 5 * steps
+    val = {k: world * units / (v / 1e3) for k, v in results.items()}
+    peak, peak_kind = measured_peaks()
+    bpd = bytes_per_dof_stage(c.N)
+    launch_ms = results["mixed"] / (5 * steps)
+    achieved = dof * bpd / (launch_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        traffic = json.load(open(prof)).get("mixed_n5_bytes_per_launch")
+    cpu = cpu_baseline(t, ph, Q0, dt, dof) if not args.no_cpu_baseline else None
+    e2e_units = dof * 5 * e2e_steps * world
+    line = {
+        "metric": METRIC,
+        "value": val["mixed"],
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": warm,
+        "ms_per_step": results["mixed"] / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 flux/f64 state",
+        "data": "synthetic",
+        "config": {
+            "workload": f"cylinder O-grid {NR}x{NT}, p={NPTS - 1} (N={NPTS}), RK_S5P3, CFL 0.3",
+            "ncell": c.mesh.ncell, "N": c.N, "dof": dof, "dt": dt,
+            "physics": f"ideal MHD gamma=5/3, Ms={MS}, MA={MA}, seeded U(+-1e-6) noise",
+            "l2": "inputs larger than L2 (236 MB per state register)",
+            "parallelism": "replicas" if world > 1 else "single GPU",
+        },
+        "fp64": {"value": val["fp64"], "ms_per_step": results["fp64"] / steps},
+        "fp64_exact": {"value": val["fp64_exact"], "ms_per_step": results["fp64_exact"] / steps},
+        "mixed_over_fp64": val["mixed"] / val["fp64"],
+        "accuracy": acc,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "bytes_per_dof_stage": bpd, "kernel": "stage_kernel<5,8,float> (mixed)"},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "e2e": {"value": e2e_units / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": int(Q0.nbytes), "d2h_bytes_per_step": int(Q0.nbytes) + 32,
+                "steps": e2e_steps, "path": "sddc_set_state + sddc_rk_step + sddc_get_state + sddc_monitor"},
+        "gpu_launches": 5 * steps,
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(t, ph, Q0, dt, dof, steps=1):
+    """The CPU oracle on all host threads, one RK3 step of the full mesh."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sddc_oracle as O
+
+    n = os.cpu_count() or 1
+    O.set_threads(n)
+    o = O.Oracle(t, ph)
+    o.set_state(Q0)
+    t0 = time.perf_counter()
+    o.rk_s5p3(dt, steps)
+    el = time.perf_counter() - t0
+    return {"value": dof * 5 * steps / el, "unit": UNIT, "cores": n, "kind": "port",
+            "sample": f"{steps} RK3 step of the {NR}x{NT} p={NPTS - 1} cylinder ({dof} DOF, 5 stages), FP64"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    c, t, Q0, dt = build_case()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sddc_oracle as O
+
+    n = os.cpu_count() or 1
+    O.set_threads(n)
+    o = O.Oracle(t, c.physics)
+    o.set_state(Q0)
+    dof = c.mesh.ncell * c.N * c.N
+    o.rk_s5p3(dt, args.warmup)
+    t0 = time.perf_counter()
+    o.rk_s5p3(dt, args.steps)
+    el = time.perf_counter() - t0
+    v = dof * 5 * args.steps / el
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"cylinder O-grid {NR}x{NT}, p={NPTS - 1} (N={NPTS}), RK_S5P3, CFL 0.3",
+                   "ncell": c.mesh.ncell, "N": c.N, "dof": dof, "dt": dt,
+                   "physics": f"ideal MHD gamma=5/3, Ms={MS}, MA={MA}"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": n, "kind": "port",
+                         "sample": f"{args.steps} full RK3 steps of the {NR}x{NT} p={NPTS - 1} cylinder; the "
+                                   "Fortran reference cannot be compiled here (no Fortran compiler), so this is "
+                                   "the C restatement of its FP64 path, OpenMP over cells and faces"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if args.steps > 10:
+            args.steps = 10  # each step is a full CPU RK3 step of 3.3M points
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,136 @@
+/*
+ * sddc.h -- C ABI of the B200 drop-in for SDDC's residual-and-time-step path.
+ *
+ * The drop-in replaces, on one GPU:
+ *   compresid                compresid.f90:1-80   (no arguments; module setup2d state)
+ *   compflux and below       compflux.f90:1-157, getrusanov.f90:1-193,
+ *                            interfaceflux_all.f90:1-112, cyclocflux_all.f90:1-112,
+ *                            bcflux.f90:1-377, AV.f90:1-142
+ *   the RK stage updates     iterations.f90:88-213 (FiveStageRk, RK_S5P3)
+ *   the monitor sums         iterations.f90:34-46
+ * The Fortran host keeps mesh input, connectivity, INIT_SETUP and calcjacob
+ * and passes their arrays here once.  The state stays on the device between
+ * calls; it crosses only when the host asks for it.
+ *
+ * Conventions:
+ *   - every array is in the reference's Fortran layout (column-major,
+ *     variable index fastest) and every index table is 1-based, exactly as
+ *     module setup2d holds it (setup2d.f90:39-102);
+ *   - the host owns every array it passes and may reuse it after the call;
+ *   - every function returns SDDC_OK (0) or a negative SDDC_E* code and
+ *     never exits; sddc_last_error() describes the last failure;
+ *   - calls on one context are serialised on the context's CUDA stream;
+ *     use one context per host thread.
+ *
+ * Fortran binding (ISO_C_BINDING) and ctypes stubs: INTEGRATION.md.
+ */
+#ifndef SDDC_H
+#define SDDC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDDC_OK 0
+#define SDDC_EINVAL (-1)      /* bad argument or inconsistent tables          */
+#define SDDC_ECUDA (-2)       /* CUDA error (message in sddc_last_error)      */
+#define SDDC_ESTATE (-3)      /* call out of order (e.g. no tables yet)       */
+#define SDDC_ENUMERIC (-4)    /* non-positive density or non-finite wave speed seen on the device */
+#define SDDC_ENOMEM (-5)      /* device allocation failed                     */
+
+/* arithmetic forms of the residual */
+#define SDDC_FP64_EXACT 0  /* the reference's FP64 operations, no FMA: bit-exact to the CPU oracle */
+#define SDDC_FP64 1        /* FP64 with FMA contraction and reciprocals (fastest FP64) */
+#define SDDC_MIXED 2       /* FP32 interpolation, fluxes and derivatives; FP64 state, RK,
+                              pressure recovery and reductions */
+
+typedef struct sddc_ctx sddc_ctx;
+
+/* Run parameters: QUAD.INP fields (readinput.f90:6-44) plus the mode. */
+typedef struct sddc_params {
+    int N;          /* solution points per direction, 2..6                     */
+    int ncell;      /* NCELL                                                   */
+    int ncellglob;  /* NCELLGLOB (AV epsilon0, AV.f90:126); 0 means ncell      */
+    int vismode;    /* 0 or 1                                                  */
+    int artiv;      /* ARTIV: 1 computes the AV sensor                         */
+    int k_stage;    /* 3: RK_S5P3, 5: FiveStageRk                              */
+    int precision;  /* SDDC_FP64_EXACT, SDDC_FP64 or SDDC_MIXED                */
+    int cells_per_cta; /* 0: default tile; else 4, 8 or 16 cells per CTA       */
+    double mu, eta0;   /* viscosity and resistivity; nonzero is rejected (see below) */
+    double dxcycl, dycycl;
+    double rinf, pinf, uinf, vinf, bxinf, byinf; /* free stream (QUAD.INP) */
+} sddc_params;
+
+/* Creates a context on the current CUDA device.  mu and eta0 must be 0:
+   with them zero the reference's viscous chain (compflux.f90:13-31) adds
+   exactly +0.0 to the residual, and this drop-in skips it. */
+int sddc_create(sddc_ctx **out, const sddc_params *p);
+void sddc_destroy(sddc_ctx *ctx);
+const char *sddc_last_error(const sddc_ctx *ctx);
+
+/* Tables from the host set-up, uploaded once (replaces the module arrays
+   read by compresid and below):
+     Lmat, Mmat (N+1,N)                       initsetup.f90:262-319
+     S1 (2,2,N+1,N,NCELL), S2 (2,2,N,N+1,NCELL), Jac (N,N,NCELL)
+                                              calcjacob.f90:1-132
+     IF2C (NFACE,4)                           connectivity.f90:153-216
+     IBFINTER(NINTER)                         connect_bdry.f90:228-244
+     IBFINL, IBFOUT, IBFWAL, IBFSYMP, IBFREE  connect_bdry.f90:126-223
+     CYC2FPAIR (NPAIR,2)                      map_cyc_loc.f90:9-35
+   Every (cell, local face) must be covered by exactly one list entry. */
+int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *Mmat, const double *S1,
+                    const double *S2, const double *Jac, const int *IF2C, int nface,
+                    const int *ibfinter, int ninter, const int *ibfinl, int ninlet,
+                    const int *ibfout, int noutlet, const int *ibfwal, int nwall,
+                    const int *ibfsymp, int nsymp, const int *ibfree, int nfree,
+                    const int *cyc2fpair, int npair);
+
+/* Q (9,N,N,NCELL) from the host, with the running maxima of the wave speed
+   and the velocity that set c_h (compflux.f90:6; both 0 at start,
+   initsetup.f90:166-167) and the solution time. */
+int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, double eigvmax, double umax);
+
+/* One residual evaluation of the current state, as compresid: keeps resid,
+   nablaQs and the AV sensor on the device and advances the running maxima. */
+int sddc_compresid(sddc_ctx *ctx);
+
+/* nsteps time steps of size dt with the scheme of k_stage (RK_S5P3 or
+   FiveStageRk), 5 residual evaluations per step.  Launches are captured in a
+   CUDA graph after the first step.  Returns SDDC_ENUMERIC if any stage saw a
+   non-positive density or a non-finite wave speed (the state is still
+   advanced, as the reference would). */
+int sddc_rk_step(sddc_ctx *ctx, double dt, int nsteps);
+
+/* Copies device results to the host; any pointer may be NULL.
+     Q (9,N,N,NCELL)
+     resid (9,N,N,NCELL), nablaQs (9,2,N,N,NCELL): from the last
+       sddc_compresid (resid also after the last stage of sddc_rk_step is
+       not kept; pass NULL then)
+     muAV (2,NCELL): AV.f90:129-140 from the last evaluation's sensor
+     sm_ind (2,NCELL): the sensor log10 values (SM_IND) */
+int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *nablaQs, double *muAV,
+                   double *sm_ind);
+
+/* Monitor sums of the last residual evaluation (iterations.f90:35-46):
+   sum of resid^2 over all variables and of divB^2; plus the integrals of
+   density and total energy (sum of Jac * w_i * w_j * Q with w the
+   quadrature weights of the solution points). */
+int sddc_monitor(sddc_ctx *ctx, double *residsum, double *divbsum, double *mass, double *energy);
+
+/* Running maxima after the last evaluation and the c_h used by the next. */
+int sddc_get_maxima(sddc_ctx *ctx, double *eigvmax, double *umax, double *c_h, double *ctime);
+
+/* Device pointer of the state (9,N,N,NCELL), valid until the next call;
+   for callers that keep their data on the GPU. */
+int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev);
+
+/* The CUDA stream (cudaStream_t) every launch of the context goes to; for
+   callers that order their own work or CUDA events against the drop-in. */
+int sddc_get_stream(sddc_ctx *ctx, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

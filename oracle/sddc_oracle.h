@@ -1,0 +1,97 @@
+/*
+ * sddc_oracle.h -- CPU restatement of SDDC's residual-and-time-step path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity oracle: tests/, the smoke
+ * check and the cpu_baseline / reference leg of bench.py may load it; the
+ * product (libsddc_b200.so and the sddc_b200 package) never does.
+ *
+ * Parity status: UNPINNED against the reference's own outputs.  The reference
+ * (chenkuangxu/SDDC, Fortran 90 + MPI) ships no tests, no golden vectors and
+ * no sample decks, and no Fortran compiler exists in this image, so the
+ * reference cannot be run to produce fixtures.  The restatement is pinned
+ * instead by mathematical known-answer tests (operator exactness, freestream
+ * preservation, Rusanov consistency, conservation, RK order) in tests/.
+ *
+ * Layout: every array uses the reference's Fortran layout (column-major,
+ * variable index fastest) and every index table is 1-based, exactly as the
+ * module setup2d (setup2d.f90:39-102) holds them.
+ */
+#ifndef SDDC_ORACLE_H
+#define SDDC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_ctx orc_ctx;
+
+typedef struct orc_params {
+    int N;            /* solution points per direction (p+1)          */
+    int ncell;        /* NCELL                                        */
+    int ncellglob;    /* NCELLGLOB (enters epsilon0, AV.f90:126)      */
+    int vismode;      /* 0 inviscid, 1 viscous chain (QUAD.INP)       */
+    int artiv;        /* ARTIV                                        */
+    int skip_ideal_viscous; /* 1: skip the viscous chain when mu==eta0==0 */
+    double mu, eta0;
+    double dxcycl, dycycl;
+    double rinf, pinf, uinf, vinf, bxinf, byinf;
+} orc_params;
+
+/* --- SD operators and metrics (initsetup.f90, mapder.f90, calcjacob.f90) */
+void orc_setsandpoints(int np, double *Xs, double *Xf);
+void orc_compute_LM(int N, const double *Xs, const double *Xf,
+                    double *Lmat, double *Mmat);
+/* bilinear metrics from 4-vertex cells (IVCELL(NCELL,4), 1-based) */
+void orc_calcjacob_bilinear(int N, int ncell, const int *ivcell,
+                            const double *xv, const double *yv,
+                            double *S1, double *S2, double *Jac);
+
+/* --- context --------------------------------------------------------- */
+orc_ctx *orc_create(const orc_params *p);
+void orc_destroy(orc_ctx *c);
+void orc_set_threads(int nthreads);
+int  orc_get_threads(void);
+/* Tables in the reference layout; the oracle copies them. */
+int orc_set_tables(orc_ctx *c, const double *Lmat, const double *Mmat,
+                   const double *S1, const double *S2, const double *Jac,
+                   const int *IF2C, int nface,
+                   const int *ibfinter, int ninter,
+                   const int *ibfinl, int ninlet,
+                   const int *ibfout, int noutlet,
+                   const int *ibfwal, int nwall,
+                   const int *ibfsymp, int nsymp,
+                   const int *ibfree, int nfree,
+                   const int *cyc2fpair, int npair);
+void orc_set_state(orc_ctx *c, const double *Q, double ctime,
+                   double eigvmax, double umax);
+void orc_get_state(const orc_ctx *c, double *Q, double *resid,
+                   double *nablaQs, double *muAV, double *sm_ind);
+void orc_get_maxima(const orc_ctx *c, double *eigvmax, double *umax,
+                    double *c_h, double *epsilon0, double *ctime);
+/* Flux arrays after the last residual (F1, G2 inviscid; Fv1, Gv2 viscous) */
+void orc_get_fluxes(const orc_ctx *c, double *F1, double *G2,
+                    double *Fv1, double *Gv2);
+
+/* --- the hot path ----------------------------------------------------- */
+void orc_compresid(orc_ctx *c);                    /* compresid.f90:1-80 */
+void orc_rk_s5p3(orc_ctx *c, double dt, int nsteps); /* iterations.f90:158-213 */
+void orc_five_stage_rk(orc_ctx *c, double dt, int nsteps); /* :88-156 */
+/* monitor sums of iterations.f90:34-46 (local, before the gather) */
+void orc_monitor(const orc_ctx *c, double *residsum, double *divbsum);
+
+/* --- point kernels, exposed for consistency tests --------------------- */
+void orc_point_iflux(const double *Qi, double c_h, double *umax,
+                     double *F, double *G);
+void orc_point_rusanov(const double *Qfl, const double *Qfr, double *Fnl,
+                       double *Fnr, const double *normf, int sign_l,
+                       int sign_r, double c_h, double *eigv,
+                       double *eigvmax, double *umax);
+/* RK_S5P3 stage combination on plain arrays (for the order test) */
+void orc_rk_s5p3_combine(int stage, long n, double dt, double *q,
+                         const double *qk0, const double *qka,
+                         const double *r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

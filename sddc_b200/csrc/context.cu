@@ -1,0 +1,649 @@
+// Host runtime of the SDDC drop-in: the C ABI of include/sddc.h.
+//
+// A context owns every device buffer of one case: the RK registers, the
+// packed metrics, the per-(cell, local face) connectivity records, the
+// running maxima and the diagnostics.  Table conversion (Fortran layout ->
+// device layout) happens once in sddc_set_tables; afterwards a time step is
+// five launches of the fused stage kernel on the context's stream, captured
+// in a CUDA graph.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sddc.h"
+#include "sd_basis.h"
+#include "stage_kernel.cuh"
+
+namespace sddc {
+cudaError_t launch_stage_exact(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
+cudaError_t launch_stage_fp64(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
+cudaError_t launch_stage_mixed(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
+}  // namespace sddc
+
+using namespace sddc;
+
+namespace {
+
+constexpr int kSlots = 5;     // rotating running-max slots
+constexpr int kRegs = 6;      // RK registers (FiveStageRk needs six)
+constexpr int kMonThreads = 256;
+
+// RK_S5P3 coefficients, iterations.f90:164-174
+constexpr double A30 = 0.355909775063327, A32 = 0.644090224936674, A40 = 0.367933791638137,
+                 A43 = 0.632066208361863, A52 = 0.237593836598569, A54 = 0.762406163401431,
+                 B10 = 0.377268915331368, B21 = 0.377268915331368, B32 = 0.242995220537396,
+                 B43 = 0.238458932846290, B54 = 0.287632146308408;
+// FiveStageRk coefficients, iterations.f90:108-150
+constexpr double F11 = 0.39175222700392, F21 = 0.44437049406734, F22 = 0.55562950593266,
+                 F23 = 0.36841059262959, F31 = 0.6201018513854, F32 = 0.3798981486146,
+                 F33 = 0.25189177424738, F41 = 0.17807995410773, F42 = 0.82192004589227,
+                 F43 = 0.54497475021237, F51 = 0.00683325884039, F52 = 0.51723167208978,
+                 F53 = 0.12759831133288, F54 = 0.34833675773694, F55 = 0.08460416338212,
+                 F56 = 0.22600748319395;
+
+// muAV from the sensor and epsilon0 (AV.f90:106-140); epsilon0 uses the
+// running max of the wave speed after the evaluation.
+__global__ void muav_kernel(int ncell, int N, double h_msh, const double *sm_ind, const double *maxima, int slot,
+                            double *muav)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const double eps0 = maxima[2 * slot] * h_msh / (double)(N - 1) * 0.05;
+    const double lo[2] = {-5.0, -3.0}, hi[2] = {0.0, 1.0};
+    for (int v = 0; v < 2; v++) {
+        const double s = sm_ind[2 * (size_t)c + v];
+        const double k = (hi[v] - lo[v]) * 0.5, s0 = (hi[v] + lo[v]) * 0.5;
+        double m;
+        if (s < lo[v]) m = 0.0;
+        else if (s > hi[v]) m = eps0;
+        else m = eps0 / 2.0 * (1.0 + sin(kPi * (s - s0) / 2.0 / k));
+        muav[2 * (size_t)c + v] = m;
+    }
+}
+
+// fixed-order sum of per-CTA partials (deterministic)
+__global__ void sum_pairs_kernel(int n, const double *part, double *out)
+{
+    __shared__ double s0[kMonThreads], s1[kMonThreads];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < n; i += kMonThreads) {
+        a += part[2 * i];
+        b += part[2 * i + 1];
+    }
+    s0[threadIdx.x] = a;
+    s1[threadIdx.x] = b;
+    __syncthreads();
+    for (int w = kMonThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s0[threadIdx.x] += s0[threadIdx.x + w];
+            s1[threadIdx.x] += s1[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s0[0];
+        out[1] = s1[0];
+    }
+}
+
+// per-cell integrals of density and energy: sum_ij Jac * w_i * w_j * Q
+__global__ void integrals_kernel(int ncell, int N, const double *q, const double *met, int met_size, int jac_off,
+                                 const double *w, double *part)
+{
+    __shared__ double s0[kMonThreads], s1[kMonThreads];
+    double a = 0.0, b = 0.0;
+    const int NN = N * N;
+    for (size_t t = blockIdx.x * (size_t)kMonThreads + threadIdx.x; t < (size_t)ncell * NN;
+         t += (size_t)gridDim.x * kMonThreads) {
+        const size_t c = t / NN;
+        const int k = (int)(t % NN), i = k % N, j = k / N;
+        const double wt = met[c * met_size + jac_off + k] * w[i] * w[j];
+        a += wt * q[9 * t];
+        b += wt * q[9 * t + 4];
+    }
+    s0[threadIdx.x] = a;
+    s1[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = kMonThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s0[threadIdx.x] += s0[threadIdx.x + s];
+            s1[threadIdx.x] += s1[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = s0[0];
+        part[2 * blockIdx.x + 1] = s1[0];
+    }
+}
+
+int met_size(int N)
+{
+    switch (N) {
+    case 2: return MetLayout<2>::kSize;
+    case 3: return MetLayout<3>::kSize;
+    case 4: return MetLayout<4>::kSize;
+    case 5: return MetLayout<5>::kSize;
+    default: return MetLayout<6>::kSize;
+    }
+}
+
+// quadrature weights of the solution points: w_i = integral over [0,1] of
+// the Lagrange basis i (moment equations sum_i w_i x_i^k = 1/(k+1))
+std::vector<double> sp_weights(const double *Xs, int N)
+{
+    std::vector<double> A(N * N), b(N);
+    for (int k = 0; k < N; k++) {
+        for (int i = 0; i < N; i++) A[k * N + i] = std::pow(Xs[i], k);
+        b[k] = 1.0 / (k + 1);
+    }
+    for (int col = 0; col < N; col++) {  // Gaussian elimination, partial pivoting
+        int piv = col;
+        for (int r = col + 1; r < N; r++)
+            if (std::fabs(A[r * N + col]) > std::fabs(A[piv * N + col])) piv = r;
+        for (int c = 0; c < N; c++) std::swap(A[col * N + c], A[piv * N + c]);
+        std::swap(b[col], b[piv]);
+        for (int r = col + 1; r < N; r++) {
+            const double f = A[r * N + col] / A[col * N + col];
+            for (int c = col; c < N; c++) A[r * N + c] -= f * A[col * N + c];
+            b[r] -= f * b[col];
+        }
+    }
+    std::vector<double> w(N);
+    for (int r = N - 1; r >= 0; r--) {
+        double s = b[r];
+        for (int c = r + 1; c < N; c++) s -= A[r * N + c] * w[c];
+        w[r] = s / A[r * N + r];
+    }
+    return w;
+}
+
+}  // namespace
+
+struct sddc_ctx {
+    sddc_params p{};
+    int N = 0, ncell = 0, cpb = 8, msize = 0, grid = 0;
+    size_t nq = 0;  // doubles per state
+    cudaStream_t stream = nullptr;
+    std::string err;
+    double *reg[kRegs] = {};
+    double *met = nullptr;
+    int2 *faces = nullptr;
+    double *maxima = nullptr;  // [kSlots][2]
+    double *sm_ind = nullptr, *muav = nullptr, *resid = nullptr, *grad = nullptr;
+    double *mon_part = nullptr, *mon_out = nullptr, *int_part = nullptr, *wq = nullptr;
+    unsigned *err_flags = nullptr;
+    double *host_small = nullptr;  // pinned scratch for small read-backs
+    Ops ops{};
+    int slot = 0;  // slot holding the running maxima after the last evaluation
+    int mon_nblk = 0;  // CTAs of the last launch that wrote monitor partials
+    bool tables = false, state = false;
+    double ctime = 0.0;
+    cudaGraphExec_t graph[kSlots] = {};
+    double graph_dt[kSlots] = {};
+};
+
+static int set_err(sddc_ctx *c, int code, const std::string &m)
+{
+    if (c) c->err = m;
+    return code;
+}
+
+static int cuda_err(sddc_ctx *c, cudaError_t e, const char *what)
+{
+    return set_err(c, SDDC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return cuda_err(ctx, e_, #call);               \
+    } while (0)
+
+extern "C" const char *sddc_last_error(const sddc_ctx *ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+static void free_all(sddc_ctx *ctx)
+{
+    for (auto &g : ctx->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    for (auto &r : ctx->reg) cudaFree(r), r = nullptr;
+    void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
+                    ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags};
+    for (void *b : bufs) cudaFree(b);
+    if (ctx->host_small) cudaFreeHost(ctx->host_small);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+}
+
+extern "C" void sddc_destroy(sddc_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+}
+
+static int alloc(sddc_ctx *ctx, void **p, size_t bytes, const char *what)
+{
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, SDDC_ENOMEM, std::string("cudaMalloc ") + what + ": " + cudaGetErrorString(e));
+    }
+    return SDDC_OK;
+}
+
+extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
+{
+    if (!out || !p) return SDDC_EINVAL;
+    *out = nullptr;
+    auto *ctx = new sddc_ctx();
+    ctx->p = *p;
+    auto bad = [&](const std::string &m) {
+        int r = set_err(ctx, SDDC_EINVAL, m);
+        *out = ctx;  // hand the context back so the caller can read the message
+        return r;
+    };
+    if (p->N < 2 || p->N > kMaxN) return bad("N must be in [2, 6]");
+    if (p->ncell < 1) return bad("ncell must be positive");
+    if (p->vismode != 0 && p->vismode != 1) return bad("vismode must be 0 or 1");
+    if (p->k_stage != 3 && p->k_stage != 5) return bad("k_stage can be only 3 or 5 (iterations.f90:22-31)");
+    if (p->precision < SDDC_FP64_EXACT || p->precision > SDDC_MIXED) return bad("unknown precision");
+    if (p->mu != 0.0 || p->eta0 != 0.0)
+        return bad("mu and eta0 must be 0: the viscous/resistive chain is not part of this drop-in");
+    if (p->cells_per_cta != 0 && p->cells_per_cta != 4 && p->cells_per_cta != 8 && p->cells_per_cta != 16)
+        return bad("cells_per_cta must be 0, 4, 8 or 16");
+    ctx->N = p->N;
+    ctx->ncell = p->ncell;
+    ctx->cpb = p->cells_per_cta ? p->cells_per_cta : 8;
+    if (!ctx->p.ncellglob) ctx->p.ncellglob = p->ncell;
+    ctx->msize = met_size(p->N);
+    ctx->nq = (size_t)9 * p->N * p->N * p->ncell;
+    ctx->grid = (p->ncell + ctx->cpb - 1) / ctx->cpb;
+    *out = ctx;
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    const int nreg = p->k_stage == 5 ? 6 : 4;
+    int rc;
+    for (int r = 0; r < nreg; r++)
+        if ((rc = alloc(ctx, (void **)&ctx->reg[r], ctx->nq * sizeof(double), "state register"))) return rc;
+    const size_t nc = p->ncell;
+    const int diag_grid = (p->ncell + 7) / 8;
+    const int mon_blocks = std::max(ctx->grid, diag_grid);
+    if ((rc = alloc(ctx, (void **)&ctx->met, nc * ctx->msize * sizeof(double), "metrics")) ||
+        (rc = alloc(ctx, (void **)&ctx->faces, nc * 4 * sizeof(int2), "faces")) ||
+        (rc = alloc(ctx, (void **)&ctx->maxima, kSlots * 2 * sizeof(double), "maxima")) ||
+        (rc = alloc(ctx, (void **)&ctx->sm_ind, nc * 2 * sizeof(double), "sensor")) ||
+        (rc = alloc(ctx, (void **)&ctx->muav, nc * 2 * sizeof(double), "muAV")) ||
+        (rc = alloc(ctx, (void **)&ctx->mon_part, (size_t)mon_blocks * 2 * sizeof(double), "monitor")) ||
+        (rc = alloc(ctx, (void **)&ctx->mon_out, 4 * sizeof(double), "monitor")) ||
+        (rc = alloc(ctx, (void **)&ctx->int_part, 1024 * 2 * sizeof(double), "integrals")) ||
+        (rc = alloc(ctx, (void **)&ctx->wq, kMaxN * sizeof(double), "weights")) ||
+        (rc = alloc(ctx, (void **)&ctx->err_flags, sizeof(unsigned), "flags")))
+        return rc;
+    CK(cudaMallocHost((void **)&ctx->host_small, 64 * sizeof(double)));
+    CK(cudaMemsetAsync(ctx->maxima, 0, kSlots * 2 * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->err_flags, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->sm_ind, 0, nc * 2 * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->mon_part, 0, (size_t)mon_blocks * 2 * sizeof(double), ctx->stream));
+
+    // operators from the SD points; Lmat/Mmat are replaced by the caller's
+    // tables in sddc_set_tables
+    const int N = p->N, NL = N - 1;
+    double Xs[kMaxN], Xf[kMaxN + 1], Xl[kMaxN], Xlf[kMaxN + 1];
+    sd_points(N, Xs, Xf);
+    sd_points(NL, Xl, Xlf);
+    for (int l = 0; l < NL; l++)
+        for (int s = 0; s < N; s++) ctx->ops.H[l * N + s] = lagrange(Xs, N, s + 1, Xl[l]);
+    for (int s = 0; s < N; s++)
+        for (int l = 0; l < NL; l++) ctx->ops.HL[s * NL + l] = lagrange(Xl, NL, l + 1, Xs[s]);
+    std::vector<double> w = sp_weights(Xs, N);
+    CK(cudaMemcpyAsync(ctx->wq, w.data(), N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SDDC_OK;
+}
+
+extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *Mmat, const double *S1,
+                               const double *S2, const double *Jac, const int *IF2C, int nface,
+                               const int *ibfinter, int ninter, const int *ibfinl, int ninlet, const int *ibfout,
+                               int noutlet, const int *ibfwal, int nwall, const int *ibfsymp, int nsymp,
+                               const int *ibfree, int nfree, const int *cyc2fpair, int npair)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (!Lmat || !Mmat || !S1 || !S2 || !Jac || !IF2C || nface < 1)
+        return set_err(ctx, SDDC_EINVAL, "sddc_set_tables: NULL table or nface < 1");
+    const int N = ctx->N, N1 = N + 1, NC = ctx->ncell;
+    for (int r = 0; r < N1; r++)
+        for (int s = 0; s < N; s++) {
+            ctx->ops.L[r * N + s] = Lmat[r + N1 * s];
+            ctx->ops.M[r * N + s] = Mmat[r + N1 * s];
+            ctx->ops.Lf[r * N + s] = (float)Lmat[r + N1 * s];
+            ctx->ops.Mf[r * N + s] = (float)Mmat[r + N1 * s];
+        }
+    // packed metrics: S1(1,1:2,r,j), S2(2,1:2,i,r), Jac(i,j)
+    std::vector<double> met((size_t)NC * ctx->msize, 0.0);
+    const int kFam = 2 * N * N1, kJac = 2 * kFam;
+    for (size_t c = 0; c < (size_t)NC; c++) {
+        double *m = &met[c * ctx->msize];
+        for (int j = 0; j < N; j++)
+            for (int r = 0; r < N1; r++) {
+                const size_t b = 4 * (r + (size_t)N1 * (j + (size_t)N * c));
+                m[2 * (j * N1 + r)] = S1[b + 0];
+                m[2 * (j * N1 + r) + 1] = S1[b + 2];
+            }
+        for (int i = 0; i < N; i++)
+            for (int r = 0; r < N1; r++) {
+                const size_t b = 4 * (i + (size_t)N * (r + (size_t)N1 * c));
+                m[kFam + 2 * (i * N1 + r)] = S2[b + 1];
+                m[kFam + 2 * (i * N1 + r) + 1] = S2[b + 3];
+            }
+        for (int k = 0; k < N * N; k++) m[kJac + k] = Jac[k + (size_t)N * N * c];
+    }
+    // per-(cell, local face) records from the reference's face lists
+    std::vector<int2> fr((size_t)NC * 4, make_int2(-1, 0));
+    auto IF2 = [&](int f, int k) { return IF2C[(f - 1) + (size_t)nface * (k - 1)]; };
+    std::string msg;
+    auto claim = [&](int cell, int lf, int partner, int kind, int plf) {
+        if (cell < 1 || cell > NC || lf < 1 || lf > 4 || (partner && (partner < 1 || partner > NC)) ||
+            (partner && (plf < 1 || plf > 4))) {
+            if (msg.empty()) msg = "face list entry out of range";
+            return;
+        }
+        int2 &r = fr[(size_t)(cell - 1) * 4 + (lf - 1)];
+        if ((r.y & 0xff) != kFaceNone) {
+            if (msg.empty())
+                msg = "cell " + std::to_string(cell) + " local face " + std::to_string(lf) + " is listed twice";
+            return;
+        }
+        r = make_int2(partner ? partner - 1 : -1, kind | (plf << 8));
+    };
+    auto face_ok = [&](int f) { return f >= 1 && f <= nface; };
+    for (int k = 0; k < ninter; k++) {
+        const int f = ibfinter[k];
+        if (!face_ok(f)) { msg = "IBFINTER entry out of range"; break; }
+        claim(IF2(f, 1), IF2(f, 3), IF2(f, 2), kFaceLeft, IF2(f, 4));
+        claim(IF2(f, 2), IF2(f, 4), IF2(f, 1), kFaceRight, IF2(f, 3));
+    }
+    for (int k = 0; k < npair && msg.empty(); k++) {
+        const int f1 = cyc2fpair[k], f2 = cyc2fpair[k + npair];
+        if (!face_ok(f1) || !face_ok(f2)) { msg = "CYC2FPAIR entry out of range"; break; }
+        claim(IF2(f1, 1), IF2(f1, 3), IF2(f2, 1), kFaceLeft, IF2(f2, 3));
+        claim(IF2(f2, 1), IF2(f2, 3), IF2(f1, 1), kFaceRight, IF2(f1, 3));
+    }
+    const int *lists[5] = {ibfinl, ibfout, ibfwal, ibfsymp, ibfree};
+    const int counts[5] = {ninlet, noutlet, nwall, nsymp, nfree};
+    const int kinds[5] = {kFaceInle, kFaceOutl, kFaceWall, kFaceSymp, kFaceFree};
+    for (int t = 0; t < 5 && msg.empty(); t++)
+        for (int k = 0; k < counts[t]; k++) {
+            const int f = lists[t][k];
+            if (!face_ok(f)) { msg = "boundary list entry out of range"; break; }
+            claim(IF2(f, 1), IF2(f, 3), 0, kinds[t], 0);
+        }
+    if (msg.empty())
+        for (size_t k = 0; k < fr.size(); k++)
+            if ((fr[k].y & 0xff) == kFaceNone) {
+                msg = "cell " + std::to_string(k / 4 + 1) + " local face " + std::to_string(k % 4 + 1) +
+                      " is in no face list (processor faces do not exist on one GPU)";
+                break;
+            }
+    if (!msg.empty()) return set_err(ctx, SDDC_EINVAL, "sddc_set_tables: " + msg);
+    CK(cudaMemcpyAsync(ctx->met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->faces, fr.data(), fr.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->tables = true;
+    return SDDC_OK;
+}
+
+extern "C" int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, double eigvmax, double umax)
+{
+    if (!ctx || !Q) return set_err(ctx, SDDC_EINVAL, "sddc_set_state: NULL argument");
+    CK(cudaMemcpyAsync(ctx->reg[0], Q, ctx->nq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    double mx[2 * kSlots];
+    for (int s = 0; s < kSlots; s++) {
+        mx[2 * s] = eigvmax;
+        mx[2 * s + 1] = umax;
+    }
+    CK(cudaMemcpyAsync(ctx->maxima, mx, sizeof(mx), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->ctime = ctime;
+    ctx->slot = 0;
+    ctx->state = true;
+    return SDDC_OK;
+}
+
+static StageArgs base_args(sddc_ctx *ctx)
+{
+    StageArgs a{};
+    a.ncell = ctx->ncell;
+    a.vismode = ctx->p.vismode;
+    a.artiv = ctx->p.artiv;
+    a.alpha = 2.0;  // initsetup.f90:165
+    a.fs = Freestream{ctx->p.rinf, ctx->p.pinf, ctx->p.uinf, ctx->p.vinf, ctx->p.bxinf, ctx->p.byinf};
+    a.met = ctx->met;
+    a.faces = ctx->faces;
+    a.maxima = ctx->maxima;
+    a.sm_ind = ctx->sm_ind;
+    a.err_flags = ctx->err_flags;
+    return a;
+}
+
+static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a)
+{
+    switch (ctx->p.precision) {
+    case SDDC_FP64_EXACT: return launch_stage_exact(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
+    case SDDC_FP64: return launch_stage_fp64(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
+    default: return launch_stage_mixed(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
+    }
+}
+
+static int ready(sddc_ctx *ctx)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (!ctx->tables) return set_err(ctx, SDDC_ESTATE, "tables not set (call sddc_set_tables)");
+    if (!ctx->state) return set_err(ctx, SDDC_ESTATE, "state not set (call sddc_set_state)");
+    return SDDC_OK;
+}
+
+static int check_flags(sddc_ctx *ctx)
+{
+    CK(cudaMemcpyAsync(ctx->host_small, ctx->err_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned f;
+    std::memcpy(&f, ctx->host_small, sizeof(unsigned));
+    if (f) {
+        CK(cudaMemsetAsync(ctx->err_flags, 0, sizeof(unsigned), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        std::string m = "device numerics:";
+        if (f & kErrNonPositiveDensity) m += " non-positive density";
+        if (f & kErrNonFiniteWaveSpeed) m += " non-finite wave speed";
+        return set_err(ctx, SDDC_ENUMERIC, m);
+    }
+    return SDDC_OK;
+}
+
+extern "C" int sddc_compresid(sddc_ctx *ctx)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    const size_t nc = ctx->ncell;
+    if (!ctx->resid) {
+        if ((rc = alloc(ctx, (void **)&ctx->resid, ctx->nq * sizeof(double), "resid")) ||
+            (rc = alloc(ctx, (void **)&ctx->grad, 2 * ctx->nq * sizeof(double), "nablaQs")))
+            return rc;
+    }
+    (void)nc;
+    StageArgs a = base_args(ctx);
+    a.rk_kind = kRkNone;
+    a.q_in = ctx->reg[0];
+    a.slot_r = ctx->slot;
+    a.slot_w = (ctx->slot + 1) % kSlots;
+    a.resid_out = ctx->resid;
+    a.grad_out = ctx->grad;
+    a.mon_part = ctx->mon_part;
+    CK(launch(ctx, true, a));
+    ctx->slot = a.slot_w;
+    ctx->mon_nblk = (ctx->ncell + 7) / 8;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_flags(ctx);
+}
+
+// the launches of one time step, starting from running-max slot s0
+static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
+{
+    double **P = ctx->reg;
+    StageArgs a = base_args(ctx);
+    struct St {
+        int kind;
+        int in, out, ra, rb, rc, rd, rw;
+        double c[6];
+    };
+    St st[5];
+    if (ctx->p.k_stage == 3) {  // RK_S5P3, iterations.f90:179-210
+        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {B10 * dt}};
+        st[1] = {kRkAxpy, 1, 2, -1, -1, -1, -1, -1, {B21 * dt}};
+        st[2] = {kRkTwoReg, 2, 1, 0, -1, -1, -1, -1, {B32 * dt, A30, A32}};
+        st[3] = {kRkTwoReg, 1, 3, 0, -1, -1, -1, -1, {B43 * dt, A40, A43}};
+        st[4] = {kRkTwoReg, 3, 0, 2, -1, -1, -1, -1, {B54 * dt, A52, A54}};
+    } else {  // FiveStageRk, iterations.f90:103-152
+        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {dt * F11}};
+        st[1] = {kRkTwoRegT, 1, 2, 0, -1, -1, -1, -1, {F23, F21, F22, dt}};
+        st[2] = {kRkTwoReg, 2, 3, 0, -1, -1, -1, -1, {F33 * dt, F31, F32}};
+        st[3] = {kRkTwoReg, 3, 4, 0, -1, -1, -1, 5, {F43 * dt, F41, F42}};
+        st[4] = {kRkFive, 4, 0, 0, 2, 3, 5, -1, {F56 * dt, F51, F52, F53, F54, F55 * dt}};
+    }
+    for (int k = 0; k < 5; k++) {
+        a.rk_kind = st[k].kind;
+        a.q_in = P[st[k].in];
+        a.q_out = P[st[k].out];
+        a.reg_a = st[k].ra >= 0 ? P[st[k].ra] : nullptr;
+        a.reg_b = st[k].rb >= 0 ? P[st[k].rb] : nullptr;
+        a.reg_c = st[k].rc >= 0 ? P[st[k].rc] : nullptr;
+        a.reg_d = st[k].rd >= 0 ? P[st[k].rd] : nullptr;
+        a.resid_w = st[k].rw >= 0 ? P[st[k].rw] : nullptr;
+        for (int i = 0; i < 6; i++) a.c[i] = st[k].c[i];
+        a.slot_r = (s0 + k) % kSlots;
+        a.slot_w = (s0 + k + 1) % kSlots;
+        a.mon_part = k == 4 ? ctx->mon_part : nullptr;
+        cudaError_t e = launch(ctx, false, a);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+extern "C" int sddc_rk_step(sddc_ctx *ctx, double dt, int nsteps)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    if (nsteps < 0) return set_err(ctx, SDDC_EINVAL, "nsteps < 0");
+    if (!(dt > 0.0)) return set_err(ctx, SDDC_EINVAL, "dt must be positive");
+    for (int s = 0; s < nsteps; s++) {
+        const int s0 = ctx->slot;
+        cudaGraphExec_t &g = ctx->graph[s0];
+        if (g && ctx->graph_dt[s0] != dt) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+        if (!g && s > 0) {  // first step of a call runs eagerly (kernel attributes, warm-up)
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = enqueue_step(ctx, dt, s0);
+            cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+            if (e != cudaSuccess) return cuda_err(ctx, e, "stage launch (capture)");
+            if (e2 != cudaSuccess) return cuda_err(ctx, e2, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&g, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_err(ctx, e, "cudaGraphInstantiate");
+            ctx->graph_dt[s0] = dt;
+        }
+        if (g) {
+            CK(cudaGraphLaunch(g, ctx->stream));
+        } else {
+            cudaError_t e = enqueue_step(ctx, dt, s0);
+            if (e != cudaSuccess) return cuda_err(ctx, e, "stage launch");
+        }
+        ctx->ctime += dt;  // ctime = ctime0 + dt after the last stage (iterations.f90:211)
+        ctx->mon_nblk = ctx->grid;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_flags(ctx);
+}
+
+extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *nablaQs, double *muAV,
+                              double *sm_ind)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (Q) CK(cudaMemcpyAsync(Q, ctx->reg[0], ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if ((resid || nablaQs) && !ctx->resid)
+        return set_err(ctx, SDDC_ESTATE, "no residual kept: call sddc_compresid first");
+    if (resid) CK(cudaMemcpyAsync(resid, ctx->resid, ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (nablaQs)
+        CK(cudaMemcpyAsync(nablaQs, ctx->grad, 2 * ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (muAV) {
+        const double h = std::sqrt(ctx->p.dxcycl * ctx->p.dycycl / (double)ctx->p.ncellglob);
+        muav_kernel<<<(ctx->ncell + 255) / 256, 256, 0, ctx->stream>>>(ctx->ncell, ctx->N, h, ctx->sm_ind,
+                                                                       ctx->maxima, ctx->slot, ctx->muav);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(muAV, ctx->muav, 2 * (size_t)ctx->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    }
+    if (sm_ind)
+        CK(cudaMemcpyAsync(sm_ind, ctx->sm_ind, 2 * (size_t)ctx->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SDDC_OK;
+}
+
+extern "C" int sddc_monitor(sddc_ctx *ctx, double *residsum, double *divbsum, double *mass, double *energy)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    sum_pairs_kernel<<<1, kMonThreads, 0, ctx->stream>>>(ctx->mon_nblk, ctx->mon_part, ctx->mon_out);
+    CK(cudaGetLastError());
+    const int ib = 1024;
+    integrals_kernel<<<ib, kMonThreads, 0, ctx->stream>>>(ctx->ncell, ctx->N, ctx->reg[0], ctx->met, ctx->msize,
+                                                          2 * (2 * ctx->N * (ctx->N + 1)), ctx->wq, ctx->int_part);
+    CK(cudaGetLastError());
+    sum_pairs_kernel<<<1, kMonThreads, 0, ctx->stream>>>(ib, ctx->int_part, ctx->mon_out + 2);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->host_small, ctx->mon_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (residsum) *residsum = ctx->host_small[0];
+    if (divbsum) *divbsum = ctx->host_small[1];
+    if (mass) *mass = ctx->host_small[2];
+    if (energy) *energy = ctx->host_small[3];
+    return SDDC_OK;
+}
+
+extern "C" int sddc_get_maxima(sddc_ctx *ctx, double *eigvmax, double *umax, double *c_h, double *ctime)
+{
+    if (!ctx) return SDDC_EINVAL;
+    CK(cudaMemcpyAsync(ctx->host_small, ctx->maxima + 2 * ctx->slot, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double e = ctx->host_small[0], u = ctx->host_small[1];
+    if (eigvmax) *eigvmax = e;
+    if (umax) *umax = u;
+    if (c_h) *c_h = std::sqrt(e * (e - u));
+    if (ctime) *ctime = ctx->ctime;
+    return SDDC_OK;
+}
+
+extern "C" int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev)
+{
+    if (!ctx || !q_dev) return SDDC_EINVAL;
+    *q_dev = ctx->reg[0];
+    return SDDC_OK;
+}
+
+extern "C" int sddc_get_stream(sddc_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return SDDC_EINVAL;
+    *stream = (void *)ctx->stream;
+    return SDDC_OK;
+}

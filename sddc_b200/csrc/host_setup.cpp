@@ -1,0 +1,416 @@
+// Host-side set-up for the SDDC residual drop-in (declared in sddc_host.h).
+//
+// Single-rank restatement of the reference host's mesh pipeline:
+//   CHECK_MESH     connectivity.f90:237-298   make every cell counter-clockwise
+//   CONNECTIVITY   connectivity.f90:1-234     faces, left/right cells, local faces
+//   CONNECT_BDRY   connect_bdry.f90:1-354     boundary lists, interior list, cyclic split
+//   MAPCYCLOC      map_cyc_loc.f90:1-42       periodic face pairs
+//   setsandpoints / computeLandM  initsetup.f90:171-344
+//   mapder / calcjacob (bilinear) mapder.f90:1-76, calcjacob.f90:1-132
+// The face numbering and the choice of left cell (the lower cell index,
+// which visits the face first) follow CONNECTIVITY, because the Rusanov flux
+// is evaluated with the left cell's metric and trace first.
+// Partitioned runs (MATCHPROC, MATCHCYCREM, processor faces) do not exist on
+// one GPU: a face that is neither interior nor on a listed boundary, or a
+// cyclic face without a partner, is an error here.
+
+#include "../../include/sddc_host.h"
+#include "sd_basis.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+constexpr double kTolCyc = 1e-5;           // tolCYC, setup2d.f90:62
+// IVFACE(IFACE,1:2): local face -> its two local vertices (connectivity.f90:73-83)
+constexpr int kIvFace[4][2] = {{1, 2}, {2, 3}, {3, 4}, {4, 1}};
+
+}  // namespace
+
+struct sddc_mesh {
+    int ncell = 0, nvert = 0, nface = 0;
+    std::vector<int> ivcell;   // (ncell,4), 1-based, CCW
+    std::vector<double> xv, yv;
+    std::vector<int> ic2f;     // (ncell,4)
+    std::vector<int> if2c;     // (nface,4)
+    std::vector<int> if2v;     // (nface,2)
+    std::vector<int> inter, inl, outl, symp, wall, cycl, freeb, cycloc, cycrem;
+    std::vector<int> pair1, pair2;
+    int nreversed = 0, nprocint = 0;
+
+    int iv(int c, int k) const { return ivcell[(c - 1) + (size_t)ncell * (k - 1)]; }
+    int &iv(int c, int k) { return ivcell[(c - 1) + (size_t)ncell * (k - 1)]; }
+};
+
+extern "C" const char *sddc_host_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------- operators
+
+using sddc::lagrange;
+using sddc::sd_points;
+
+extern "C" int sddc_sd_operators(int N, double *Xs, double *Xf, double *Lmat, double *Mmat)
+{
+    if (N < 2 || N > 6) return fail(-1, "sddc_sd_operators: N must be in [2, 6]");
+    sd_points(N, Xs, Xf);
+    const int N1 = N + 1;
+    for (int f = 1; f <= N1; f++)
+        for (int s = 1; s <= N; s++) Lmat[(f - 1) + N1 * (s - 1)] = lagrange(Xs, N, s, Xf[f - 1]);
+    // derivative of the flux-point basis at the solution points, written as
+    // the sum over k of the product rule terms (computeLandM)
+    for (int f = 1; f <= N1; f++)
+        for (int s = 1; s <= N; s++) {
+            const double x = Xs[s - 1];
+            double acc = 0.0;
+            for (int k = 1; k <= N1; k++) {
+                if (k == f) continue;
+                double num = 1.0, den = 1.0;
+                for (int q = 1; q <= N1; q++) {
+                    if (q != f && q != k) num = num * (x - Xf[q - 1]);
+                    if (q != f) den = den * (Xf[f - 1] - Xf[q - 1]);
+                }
+                acc = acc + num / den;
+            }
+            Mmat[(f - 1) + N1 * (s - 1)] = acc;
+        }
+    return 0;
+}
+
+// ---------------------------------------------------------------- mesh
+
+static int build_mesh(sddc_mesh &m, const int *bnd_v, const int *bnd_type, int nbound,
+                      double dxcycl, double dycycl)
+{
+    const int NC = m.ncell, NVERT = m.nvert;
+    // CHECK_MESH: signed shoelace sum; positive means clockwise -> swap 1<->2, 3<->4
+    for (int c = 1; c <= NC; c++) {
+        double sum = 0.0;
+        for (int f = 0; f < 4; f++) {
+            int a = m.iv(c, kIvFace[f][0]), b = m.iv(c, kIvFace[f][1]);
+            sum += (m.xv[b - 1] - m.xv[a - 1]) * (m.yv[a - 1] + m.yv[b - 1]);
+        }
+        if (sum > 0) {
+            int v1 = m.iv(c, 1), v2 = m.iv(c, 2), v3 = m.iv(c, 3), v4 = m.iv(c, 4);
+            m.iv(c, 1) = v2; m.iv(c, 2) = v1; m.iv(c, 3) = v4; m.iv(c, 4) = v3;
+            m.nreversed++;
+        }
+    }
+    // vertex -> cells (CSR in cell order)
+    std::vector<int> start(NVERT + 2, 0), fillc(NVERT + 1, 0);
+    for (int c = 1; c <= NC; c++)
+        for (int k = 1; k <= 4; k++) {
+            int v = m.iv(c, k);
+            if (v < 1 || v > NVERT) return fail(-2, "vertex index out of range in IVCELL");
+            fillc[v]++;
+        }
+    for (int v = 1; v <= NVERT; v++)
+        if (fillc[v] == 0) return fail(-3, "vertex " + std::to_string(v) + " belongs to no cell");
+    start[1] = 0;
+    for (int v = 1; v <= NVERT; v++) start[v + 1] = start[v] + fillc[v];
+    std::vector<int> cells(start[NVERT + 1]);
+    {
+        std::vector<int> pos(start.begin(), start.end());
+        for (int c = 1; c <= NC; c++)
+            for (int k = 1; k <= 4; k++) cells[pos[m.iv(c, k)]++] = c;
+    }
+    // CONNECTIVITY: the first cell to visit a face is its left cell
+    m.ic2f.assign((size_t)NC * 4, 0);
+    std::vector<int> fl, fr, fv1, fv2;
+    fl.reserve((size_t)NC * 2 + 8);
+    auto ic2f = [&](int c, int f) -> int & { return m.ic2f[(c - 1) + (size_t)NC * (f - 1)]; };
+    for (int c = 1; c <= NC; c++) {
+        for (int f = 1; f <= 4; f++) {
+            if (ic2f(c, f) != 0) continue;
+            const int vb = m.iv(c, kIvFace[f - 1][0]), v1 = m.iv(c, kIvFace[f - 1][1]);
+            int nb = 0, nbf = 0;
+            for (int k = start[vb]; k < start[vb + 1] && !nb; k++) {
+                int cc = cells[k];
+                if (cc == c) continue;
+                for (int ff = 1; ff <= 4; ff++) {
+                    int a = m.iv(cc, kIvFace[ff - 1][0]), b = m.iv(cc, kIvFace[ff - 1][1]);
+                    if ((vb == a && v1 == b) || (vb == b && v1 == a)) {
+                        nb = cc;
+                        nbf = ff;
+                        break;
+                    }
+                }
+            }
+            fl.push_back(c);
+            fr.push_back(nb);
+            fv1.push_back(vb);
+            fv2.push_back(v1);
+            const int face = (int)fl.size();
+            if (nb) ic2f(nb, nbf) = face;
+            ic2f(c, f) = face;
+        }
+    }
+    const int NF = (int)fl.size();
+    m.nface = NF;
+    m.if2c.assign((size_t)NF * 4, 0);
+    m.if2v.assign((size_t)NF * 2, 0);
+    auto IF2C = [&](int f, int k) -> int & { return m.if2c[(f - 1) + (size_t)NF * (k - 1)]; };
+    for (int f = 1; f <= NF; f++) {
+        IF2C(f, 1) = fl[f - 1];
+        IF2C(f, 2) = fr[f - 1];
+        m.if2v[f - 1] = fv1[f - 1];
+        m.if2v[(f - 1) + NF] = fv2[f - 1];
+    }
+    // local face of the left cell from the face's vertex sequence, and of
+    // the right cell from the reversed sequence
+    for (int f = 1; f <= NF; f++) {
+        const int a = fv1[f - 1], b = fv2[f - 1];
+        const int c1 = IF2C(f, 1), c2 = IF2C(f, 2);
+        for (int lf = 1; lf <= 4 && !IF2C(f, 3); lf++)
+            if (m.iv(c1, kIvFace[lf - 1][0]) == a && m.iv(c1, kIvFace[lf - 1][1]) == b) IF2C(f, 3) = lf;
+        if (!IF2C(f, 3)) return fail(-4, "connectivity: face " + std::to_string(f) + " not on its left cell");
+        if (c2) {
+            for (int lf = 1; lf <= 4 && !IF2C(f, 4); lf++)
+                if (m.iv(c2, kIvFace[lf - 1][1]) == a && m.iv(c2, kIvFace[lf - 1][0]) == b) IF2C(f, 4) = lf;
+            if (!IF2C(f, 4))
+                return fail(-4, "connectivity: face " + std::to_string(f) +
+                                    " has the same orientation in both cells");
+        }
+    }
+    // CONNECT_BDRY: attach each boundary record to its face
+    std::vector<char> is_bnd(NF + 1, 0);
+    for (int ib = 0; ib < nbound; ib++) {
+        const int vb1 = bnd_v[ib], vb3 = bnd_v[ib + nbound];
+        if (vb1 < 1 || vb1 > NVERT || vb3 < 1 || vb3 > NVERT)
+            return fail(-5, "boundary record " + std::to_string(ib + 1) + ": vertex out of range");
+        int icc = 0;  // last cell touching both vertices, as the reference's double loop
+        for (int k1 = start[vb1]; k1 < start[vb1 + 1]; k1++)
+            for (int k3 = start[vb3]; k3 < start[vb3 + 1]; k3++)
+                if (cells[k1] == cells[k3]) icc = cells[k1];
+        if (!icc) return fail(-5, "boundary record " + std::to_string(ib + 1) + " touches no cell");
+        int face = 0;
+        for (int lf = 1; lf <= 4; lf++) {
+            int a = m.iv(icc, kIvFace[lf - 1][0]), b = m.iv(icc, kIvFace[lf - 1][1]);
+            if ((a == vb1 || b == vb1) && (a == vb3 || b == vb3)) {
+                face = ic2f(icc, lf);
+                break;
+            }
+        }
+        if (!face) return fail(-5, "boundary record " + std::to_string(ib + 1) + " is not a cell face");
+        is_bnd[face] = 1;
+        switch (bnd_type[ib]) {
+        case SDDC_BC_INLE: m.inl.push_back(face); break;
+        case SDDC_BC_OUTL: m.outl.push_back(face); break;
+        case SDDC_BC_SYMP: m.symp.push_back(face); break;
+        case SDDC_BC_WALL: m.wall.push_back(face); break;
+        case SDDC_BC_CYCL: m.cycl.push_back(face); break;
+        case SDDC_BC_FREE: m.freeb.push_back(face); break;
+        default: return fail(-6, "boundary record " + std::to_string(ib + 1) + ": unknown type");
+        }
+    }
+    for (int f = 1; f <= NF; f++) {
+        if (IF2C(f, 2) != 0) m.inter.push_back(f);
+        else if (!is_bnd[f]) m.nprocint++;
+    }
+    if (m.nprocint)
+        return fail(-7, std::to_string(m.nprocint) +
+                            " boundary faces carry no boundary condition (processor faces do not "
+                            "exist on one GPU)");
+    // cyclic faces: local when a translated partner exists (connect_bdry.f90:281-308)
+    auto mid = [&](int f, double &x, double &y) {
+        int a = m.if2v[f - 1], b = m.if2v[(f - 1) + NF];
+        x = (m.xv[a - 1] + m.xv[b - 1]) / 2;
+        y = (m.yv[a - 1] + m.yv[b - 1]) / 2;
+    };
+    auto matches = [&](int f1, int f2) {
+        double x1, y1, x2, y2;
+        mid(f1, x1, y1);
+        mid(f2, x2, y2);
+        double ex = std::fabs(std::fabs(x1 - x2) - dxcycl), ey = std::fabs(std::fabs(y1 - y2) - dycycl);
+        return (std::fabs(x1 - x2) < kTolCyc && ey < kTolCyc) || (std::fabs(y1 - y2) < kTolCyc && ex < kTolCyc);
+    };
+    for (int f : m.cycl) {
+        bool found = false;
+        for (int g : m.cycl)
+            if (matches(f, g)) { found = true; break; }
+        (found ? m.cycloc : m.cycrem).push_back(f);
+    }
+    if (!m.cycrem.empty())
+        return fail(-8, std::to_string(m.cycrem.size()) + " cyclic faces have no periodic partner");
+    // MAPCYCLOC: pair each local cyclic face with a later one
+    for (size_t i = 0; i < m.cycloc.size(); i++)
+        for (size_t j = i + 1; j < m.cycloc.size(); j++)
+            if (matches(m.cycloc[i], m.cycloc[j])) {
+                m.pair1.push_back(m.cycloc[i]);
+                m.pair2.push_back(m.cycloc[j]);
+            }
+    if (m.pair1.size() * 2 != m.cycloc.size())
+        return fail(-9, "cyclic faces do not pair up (" + std::to_string(m.pair1.size()) + " pairs for " +
+                            std::to_string(m.cycloc.size()) + " faces)");
+    return 0;
+}
+
+extern "C" int sddc_mesh_build(sddc_mesh **out, int ncell, int nvert, const int *ivcell, const double *xv,
+                               const double *yv, int nbound, const int *bnd_v, const int *bnd_type,
+                               double dxcycl, double dycycl)
+{
+    if (!out) return fail(-1, "sddc_mesh_build: out is NULL");
+    *out = nullptr;
+    if (ncell < 1 || nvert < 4 || !ivcell || !xv || !yv || nbound < 0 || (nbound && (!bnd_v || !bnd_type)))
+        return fail(-1, "sddc_mesh_build: bad arguments");
+    auto *m = new sddc_mesh();
+    m->ncell = ncell;
+    m->nvert = nvert;
+    m->ivcell.assign(ivcell, ivcell + (size_t)ncell * 4);
+    m->xv.assign(xv, xv + nvert);
+    m->yv.assign(yv, yv + nvert);
+    int rc = build_mesh(*m, bnd_v, bnd_type, nbound, dxcycl, dycycl);
+    if (rc) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return 0;
+}
+
+extern "C" void sddc_mesh_destroy(sddc_mesh *m) { delete m; }
+
+extern "C" int sddc_mesh_counts(const sddc_mesh *m, int *c)
+{
+    if (!m || !c) return fail(-1, "sddc_mesh_counts: NULL argument");
+    c[SDDC_MC_NFACE] = m->nface;
+    c[SDDC_MC_NINTER] = (int)m->inter.size();
+    c[SDDC_MC_NINLET] = (int)m->inl.size();
+    c[SDDC_MC_NOUTLET] = (int)m->outl.size();
+    c[SDDC_MC_NSYMP] = (int)m->symp.size();
+    c[SDDC_MC_NWALL] = (int)m->wall.size();
+    c[SDDC_MC_NCYCL] = (int)m->cycl.size();
+    c[SDDC_MC_NCYCLOC] = (int)m->cycloc.size();
+    c[SDDC_MC_NCYCREM] = (int)m->cycrem.size();
+    c[SDDC_MC_NPAIR] = (int)m->pair1.size();
+    c[SDDC_MC_NPROCINT] = m->nprocint;
+    c[SDDC_MC_NFREE] = (int)m->freeb.size();
+    c[SDDC_MC_NREVERSED] = m->nreversed;
+    c[SDDC_MC_NVERT] = m->nvert;
+    c[SDDC_MC_NCELL] = m->ncell;
+    return 0;
+}
+
+static void copy_list(const std::vector<int> &v, int *dst)
+{
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), sizeof(int) * v.size());
+}
+
+extern "C" int sddc_mesh_tables(const sddc_mesh *m, int *if2c, int *if2v, int *ibfinter, int *ibfinl,
+                                int *ibfout, int *ibfwal, int *ibfsymp, int *ibfree, int *cyc2fpair,
+                                int *ivcell_ccw)
+{
+    if (!m) return fail(-1, "sddc_mesh_tables: NULL mesh");
+    copy_list(m->if2c, if2c);
+    copy_list(m->if2v, if2v);
+    copy_list(m->inter, ibfinter);
+    copy_list(m->inl, ibfinl);
+    copy_list(m->outl, ibfout);
+    copy_list(m->wall, ibfwal);
+    copy_list(m->symp, ibfsymp);
+    copy_list(m->freeb, ibfree);
+    copy_list(m->ivcell, ivcell_ccw);
+    if (cyc2fpair) {
+        const size_t np = m->pair1.size();
+        for (size_t i = 0; i < np; i++) {
+            cyc2fpair[i] = m->pair1[i];
+            cyc2fpair[i + np] = m->pair2[i];
+        }
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- metrics
+
+// derivatives of the four bilinear shape functions at (psi, eta) (mapder)
+static void shape_derivs(double psi, double eta, double d[4][2])
+{
+    d[0][0] = eta - 1.0; d[0][1] = psi - 1.0;
+    d[1][0] = 1.0 - eta; d[1][1] = -psi;
+    d[2][0] = eta;       d[2][1] = psi;
+    d[3][0] = -eta;      d[3][1] = 1.0 - psi;
+}
+
+struct Derivs {
+    double xpsi, ypsi, xeta, yeta;
+};
+
+static Derivs map_derivs(const double X[4], const double Y[4], double psi, double eta)
+{
+    double d[4][2];
+    shape_derivs(psi, eta, d);
+    Derivs r{0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < 4; k++) {
+        r.xpsi = r.xpsi + d[k][0] * X[k];
+        r.ypsi = r.ypsi + d[k][0] * Y[k];
+        r.xeta = r.xeta + d[k][1] * X[k];
+        r.yeta = r.yeta + d[k][1] * Y[k];
+    }
+    return r;
+}
+
+extern "C" int sddc_mesh_metrics(const sddc_mesh *m, int N, double *S1, double *S2, double *Jac, double *xxsolu)
+{
+    if (!m) return fail(-1, "sddc_mesh_metrics: NULL mesh");
+    if (N < 2 || N > 6) return fail(-1, "sddc_mesh_metrics: N must be in [2, 6]");
+    double Xs[8], Xf[8];
+    sd_points(N, Xs, Xf);
+    const int N1 = N + 1;
+    for (int c = 1; c <= m->ncell; c++) {
+        double X[4], Y[4];
+        for (int k = 1; k <= 4; k++) {
+            X[k - 1] = m->xv[m->iv(c, k) - 1];
+            Y[k - 1] = m->yv[m->iv(c, k) - 1];
+        }
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++) {
+                Derivs d = map_derivs(X, Y, Xs[i - 1], Xs[j - 1]);
+                if (Jac) Jac[(i - 1) + (size_t)N * ((j - 1) + (size_t)N * (c - 1))] = d.xpsi * d.yeta - d.xeta * d.ypsi;
+                if (xxsolu) {
+                    // xyCoor_atGps with MapBaseFunc (mapder.f90:79-87, 255-273)
+                    const double xi = Xs[i - 1], et = Xs[j - 1];
+                    const double fn[4] = {(1.0 - xi) * (1.0 - et), (1.0 - et) * xi, xi * et, (1.0 - xi) * et};
+                    double px = 0.0, py = 0.0;
+                    for (int k = 0; k < 4; k++) {
+                        px = px + X[k] * fn[k];
+                        py = py + Y[k] * fn[k];
+                    }
+                    size_t b = 2 * ((i - 1) + (size_t)N * ((j - 1) + (size_t)N * (c - 1)));
+                    xxsolu[b] = px;
+                    xxsolu[b + 1] = py;
+                }
+            }
+        if (S1)
+            for (int j = 1; j <= N; j++)
+                for (int f = 1; f <= N1; f++) {
+                    Derivs d = map_derivs(X, Y, Xf[f - 1], Xs[j - 1]);
+                    size_t b = 4 * ((f - 1) + (size_t)N1 * ((j - 1) + (size_t)N * (c - 1)));
+                    S1[b + 0] = d.yeta;   // S1(1,1)
+                    S1[b + 1] = -d.ypsi;  // S1(2,1)
+                    S1[b + 2] = -d.xeta;  // S1(1,2)
+                    S1[b + 3] = d.xpsi;   // S1(2,2)
+                }
+        if (S2)
+            for (int f = 1; f <= N1; f++)
+                for (int i = 1; i <= N; i++) {
+                    Derivs d = map_derivs(X, Y, Xs[i - 1], Xf[f - 1]);
+                    size_t b = 4 * ((i - 1) + (size_t)N * ((f - 1) + (size_t)N1 * (c - 1)));
+                    S2[b + 0] = d.yeta;
+                    S2[b + 1] = -d.ypsi;
+                    S2[b + 2] = -d.xeta;
+                    S2[b + 3] = d.xpsi;
+                }
+    }
+    return 0;
+}

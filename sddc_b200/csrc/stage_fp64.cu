@@ -1,0 +1,5 @@
+// FP64 form of the stage kernel with FMA contraction and reciprocals.
+#define SDDC_R double
+#define SDDC_EXACT_FORM false
+#define SDDC_LAUNCH launch_stage_fp64
+#include "stage_launch.inc"

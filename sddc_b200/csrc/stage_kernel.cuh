@@ -1,0 +1,538 @@
+// The fused residual + RK stage kernel of the SDDC drop-in.
+//
+// One launch evaluates compresid (compresid.f90:1-80, compflux.f90:1-104,
+// interfaceflux_all.f90:1-112, cyclocflux_all.f90:1-112, bcflux.f90:1-377,
+// nablaQsp compflux.f90:107-157, the AV sensor AV.f90:1-142) for every cell
+// and applies one RK stage update (iterations.f90:88-213) to it, so a stage
+// reads the state once and writes it once.
+//
+// Work split: one CTA owns CPB consecutive cells and stages them in shared
+// memory.  Phases, separated by __syncthreads:
+//   A  Lagrange interpolation of every line of solution points to its N+1
+//      flux points (one thread per cell x family x line x variable);
+//   B1 physical flux at the interior flux points (thread per point);
+//   B2 Rusanov flux at the 4N face points of each cell (thread per point).
+//      The neighbour's trace is interpolated from the neighbour's state in
+//      global memory (served by L2; neighbours are a few cells away in
+//      memory).  Each shared face is evaluated by both of its cells, each
+//      with the reference's left/right assignment, so both get the value
+//      the reference scatters to them;
+//   C  divergence of the flux, gradient of (Bx, By) from the face-averaged
+//      flux-point states, Powell and GLM sources and the RK update (thread
+//      per solution point);
+//   D  the AV smoothness sensor per cell.
+// Running maxima of the wave speed and of the velocity (the c_h input of
+// the next stage) go through atomicMax on five rotating slots, so that
+// launches need no host synchronisation.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "physics.cuh"
+
+namespace sddc {
+
+constexpr int kMaxN = 6;
+
+// threads of a CTA owning cpb cells: 4N per cell (one per face point),
+// rounded up to whole warps
+__host__ __device__ constexpr int stage_threads(int n, int cpb) { return (4 * n * cpb + 31) / 32 * 32; }
+
+// operators in kernel parameter space (row-major)
+struct Ops {
+    double L[(kMaxN + 1) * kMaxN];   // L[r*N + s]  = Lmat(r+1, s+1)
+    double M[(kMaxN + 1) * kMaxN];   // M[r*N + s]  = Mmat(r+1, s+1)
+    double H[(kMaxN - 1) * kMaxN];   // H[l*N + s]  = hhval(s+1, Xs_low(l+1))
+    double HL[kMaxN * (kMaxN - 1)];  // HL[s*(N-1) + l] = hhval_low(l+1, Xs(s+1))
+    float Lf[(kMaxN + 1) * kMaxN];
+    float Mf[(kMaxN + 1) * kMaxN];
+};
+
+// how the stage output is formed from the residual r of the stage input q
+enum RkKind : int {
+    kRkNone = 0,     // residual evaluation only (compresid)
+    kRkAxpy = 1,     // out = q + c0*r                                     RK_S5P3 stages 1-2, FiveStageRk stage 1
+    kRkTwoReg = 2,   // out = (c1*a + c2*q) + c0*r                         RK_S5P3 stages 3-5, FiveStageRk stages 3-4
+    kRkTwoRegT = 3,  // out = (c1*a + c2*q) + (c0*r)*c3                    FiveStageRk stage 2
+    kRkFive = 4      // out = ((((c1*a + c2*b) + c3*c) + c4*q) + c5*d) + c0*r   FiveStageRk stage 5
+};
+
+struct StageArgs {
+    int ncell;
+    int vismode;
+    int artiv;
+    int rk_kind;
+    int slot_r, slot_w;
+    double alpha;
+    double c[8];
+    Freestream fs;
+    const double *__restrict__ q_in;   // (9,N,N,NCELL), never written during the stage
+    double *q_out;                     // RK output (may be reg_a: FiveStageRk stage 5)
+    const double *reg_a;               // RK registers read by this stage
+    const double *reg_b;
+    const double *reg_c;
+    const double *reg_d;
+    double *resid_w;                   // residual copy (FiveStageRk stage 4 resid0)
+    const double *__restrict__ met;    // packed metrics, per cell
+    const int2 *__restrict__ faces;    // (cell, local face) records
+    double *maxima;                    // [5][2]: running max of eigv, umax
+    double *__restrict__ sm_ind;       // (2,NCELL) AV sensor
+    double *__restrict__ resid_out;    // (9,N,N,NCELL), residual evaluation only
+    double *__restrict__ grad_out;     // (9,2,N,N,NCELL), residual evaluation only
+    double *__restrict__ mon_part;     // per-CTA (sum resid^2, sum divB^2), or null
+    unsigned *err_flags;
+};
+
+// packed per-cell metric record: normals of both flux-point families, then Jac
+template <int N> struct MetLayout {
+    static constexpr int kFam = 2 * N * (N + 1);       // doubles per family
+    static constexpr int kJac = 2 * kFam;              // offset of Jac(i,j) at kJac + i + N*j
+    static constexpr int kSize = (2 * kFam + N * N + 1) & ~1;
+    // normal (S1(1,1:2) or S2(2,1:2)) of family f, line l, flux point r
+    __host__ __device__ static constexpr int normal(int f, int l, int r) { return f * kFam + 2 * (l * (N + 1) + r); }
+};
+
+// error flag bits
+enum : unsigned { kErrNonPositiveDensity = 1u, kErrNonFiniteWaveSpeed = 2u };
+
+template <int N, typename R, bool DIAG> struct Smem {
+    static constexpr int NQ = 9 * N * N;
+    static constexpr int NP = N + 1;
+    static constexpr int NG = DIAG ? 9 : 2;  // variables of the face-averaged state kept for gradients
+    static constexpr int kF = 2 * N * NP * 9;   // R per cell: state then flux at every flux point
+    static constexpr int kV = 2 * N * NP * NG;  // R per cell: face-averaged state at every flux point
+    static constexpr int kLow = 2 * (N - 1) * (N - 1);
+};
+
+// Lagrange coefficient access in the arithmetic type
+template <typename R> __device__ __forceinline__ R opL(const Ops &o, int i);
+template <> __device__ __forceinline__ double opL<double>(const Ops &o, int i) { return o.L[i]; }
+template <> __device__ __forceinline__ float opL<float>(const Ops &o, int i) { return o.Lf[i]; }
+template <typename R> __device__ __forceinline__ R opM(const Ops &o, int i);
+template <> __device__ __forceinline__ double opM<double>(const Ops &o, int i) { return o.M[i]; }
+template <> __device__ __forceinline__ float opM<float>(const Ops &o, int i) { return o.Mf[i]; }
+
+// local face lf (1..4), face point nfp (1..N) -> flux point (family, line, point)
+// (face2fpconnec, initsetup.f90:347-383)
+template <int N>
+__device__ __forceinline__ void face_point(int lf, int nfp, int &fam, int &line, int &r)
+{
+    switch (lf) {
+    case 1: fam = 1; line = nfp - 1; r = 0; break;       // (nfp, 1)
+    case 2: fam = 0; line = nfp - 1; r = N; break;       // (N+1, nfp)
+    case 3: fam = 1; line = N - nfp; r = N; break;       // (N-nfp+1, N+1)
+    default: fam = 0; line = N - nfp; r = 0; break;      // (1, N-nfp+1)
+    }
+}
+
+template <typename T> __device__ __forceinline__ T warp_max(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// EXACT instantiations are compiled without FMA contraction (-fmad=false) in
+// their own translation unit; they reproduce the reference's FP64 rounding.
+template <int N, int CPB, typename R, bool DIAG, bool EXACT>
+__global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const StageArgs a, const Ops ops)
+{
+    constexpr bool EX = EXACT && (sizeof(R) == sizeof(double));
+    using S = Smem<N, R, DIAG>;
+    using ML = MetLayout<N>;
+    constexpr int NT = stage_threads(N, CPB);  // whole warps: the reductions use full-warp masks
+    constexpr int NQ = S::NQ, NP = S::NP, NG = S::NG;
+    constexpr int NN = N * N;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sQ = reinterpret_cast<double *>(smem_raw);          // [CPB][NQ]
+    double *sMet = sQ + CPB * NQ;                                // [CPB][ML::kSize]
+    double *sJz = sMet + CPB * ML::kSize;                        // [CPB][NN]  Jz^2 for the sensor
+    double *sLow = sJz + CPB * NN;                               // [CPB][kLow]
+    double *sRed = sLow + CPB * S::kLow;                         // [4][32] block reductions
+    R *sF = reinterpret_cast<R *>(sRed + 4 * 32);                // [CPB][2][N][NP][9]
+    R *sV = sF + CPB * S::kF;                                    // [CPB][2][N][NP][NG]
+    R *sQr = sV + CPB * S::kV;                                   // [CPB][NQ] (float form only)
+
+    const int tid = threadIdx.x;
+    const int c0 = blockIdx.x * CPB;
+    const int ncl = min(CPB, a.ncell - c0);  // cells of this CTA
+
+    // ---- stage the state and the metrics ------------------------------------
+    {
+        const double *src = a.q_in + (size_t)c0 * NQ;
+        const int n = ncl * NQ;
+        for (int k = tid; k < n; k += NT) sQ[k] = __ldg(src + k);
+        const double *msrc = a.met + (size_t)c0 * ML::kSize;
+        const int nm = ncl * ML::kSize;
+        for (int k = tid; k < nm; k += NT) sMet[k] = __ldg(msrc + k);
+    }
+    const double eig_r = a.maxima[2 * a.slot_r], um_r = a.maxima[2 * a.slot_r + 1];
+    // compflux.f90:6 -- running maxima of all previous stages
+    const R c_h = (R)sqrt(eig_r * (eig_r - um_r));
+    __syncthreads();
+    if constexpr (sizeof(R) != sizeof(double)) {
+        for (int k = tid; k < ncl * NQ; k += NT) sQr[k] = (R)sQ[k];
+        __syncthreads();
+    }
+    const R *qsrc = (sizeof(R) == sizeof(double)) ? reinterpret_cast<const R *>(sQ) : sQr;
+
+    // ---- A: interpolate every line to its flux points ---------------------------
+    for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
+        const int v = t % 9, l = (t / 9) % N, f = (t / (9 * N)) % 2, c = t / (18 * N);
+        const R *q = qsrc + c * NQ;
+        R qs[N];
+#pragma unroll
+        for (int s = 0; s < N; s++) qs[s] = f == 0 ? q[v + 9 * (s + N * l)] : q[v + 9 * (l + N * s)];
+        R *out = sF + c * S::kF + (f * N + l) * NP * 9 + v;
+#pragma unroll
+        for (int r = 0; r < NP; r++) {
+            R acc = (R)0;
+#pragma unroll
+            for (int s = 0; s < N; s++) acc = acc + qs[s] * opL<R>(ops, r * N + s);
+            out[r * 9] = acc;
+        }
+    }
+    __syncthreads();
+
+    R eigmax = (R)0, umax = (R)0;
+    unsigned err = 0;
+
+    // ---- B1: interior flux points (inviscid_flux_interior) ---------------------
+    for (int t = tid; t < ncl * 2 * N * (N - 1); t += NT) {
+        const int r = 1 + t % (N - 1), l = (t / (N - 1)) % N, f = (t / ((N - 1) * N)) % 2,
+                  c = t / (2 * N * (N - 1));
+        R *slot = sF + c * S::kF + ((f * N + l) * NP + r) * 9;
+        R q[9], F[9], G[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = slot[k];
+        if (!(q[0] > (R)0)) err |= kErrNonPositiveDensity;
+        iflux<R, EX>(q, c_h, umax, F, G);
+        const double *nrm = sMet + c * ML::kSize + ML::normal(f, l, r);
+        const R n0 = (R)nrm[0], n1 = (R)nrm[1];
+#pragma unroll
+        for (int k = 0; k < 9; k++) slot[k] = F[k] * n0 + G[k] * n1;
+        R *vs = sV + c * S::kV + ((f * N + l) * NP + r) * NG;
+        if constexpr (DIAG) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) vs[k] = q[k];
+        } else {
+            vs[0] = q[5];
+            vs[1] = q[6];
+        }
+    }
+
+    // ---- B2: face points (interfaceflux, CYCLOCFLUX, BCFLUX) -------------------
+    for (int t = tid; t < ncl * 4 * N; t += NT) {
+        const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
+        int fam, line, r;
+        face_point<N>(lf, nfp, fam, line, r);
+        R *slot = sF + c * S::kF + ((fam * N + line) * NP + r) * 9;
+        R own[9], other[9], Fl[9], Fr[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) own[k] = slot[k];
+        const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
+        const int kind = rec.y & 0xff;
+        const double *onrm = sMet + c * ML::kSize + ML::normal(fam, line, r);
+        const R *Ql, *Qr;
+        R n0, n1;
+        int sign_l, sign_r;
+        if (kind == kFaceLeft || kind == kFaceRight) {
+            // partner point N-nfp+1 on the partner's local face
+            const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
+            int pfam, pline, pr;
+            face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
+            const double *qp = a.q_in + (size_t)pc * NQ + (pfam == 0 ? 9 * N * pline : 9 * pline);
+            const int stride = pfam == 0 ? 9 : 9 * N;
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                R acc = (R)0;
+#pragma unroll
+                for (int s = 0; s < N; s++) acc = acc + (R)__ldg(qp + k + stride * s) * opL<R>(ops, pr * N + s);
+                other[k] = acc;
+            }
+            if (kind == kFaceLeft) {
+                Ql = own; Qr = other;
+                n0 = (R)onrm[0]; n1 = (R)onrm[1];
+                sign_l = r == 0 ? -1 : 1;
+                sign_r = pr == N ? -1 : 1;
+            } else {
+                Ql = other; Qr = own;
+                const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
+                n0 = (R)__ldg(pn);
+                n1 = (R)__ldg(pn + 1);
+                sign_l = pr == 0 ? -1 : 1;
+                sign_r = r == N ? -1 : 1;
+            }
+        } else {
+            n0 = (R)onrm[0]; n1 = (R)onrm[1];
+            sign_l = r == 0 ? -1 : 1;
+            sign_r = 1;
+            bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.fs, other);
+            Ql = own; Qr = other;
+        }
+        if (!(Ql[0] > (R)0) || !(Qr[0] > (R)0)) err |= kErrNonPositiveDensity;
+        R eig_face;
+        rusanov<R, EX>(Ql, Qr, Fl, Fr, n0, n1, sign_l, sign_r, c_h, eig_face, umax);
+        if (!(Abs<R>(eig_face) < (R)INFINITY)) err |= kErrNonFiniteWaveSpeed;
+        if (eig_face > eigmax) eigmax = eig_face;
+        const R *fo = (kind == kFaceRight) ? Fr : Fl;
+#pragma unroll
+        for (int k = 0; k < 9; k++) slot[k] = fo[k];
+        R *vs = sV + c * S::kV + ((fam * N + line) * NP + r) * NG;
+        if constexpr (DIAG) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) vs[k] = (R)0.5 * Ql[k] + (R)0.5 * Qr[k];
+        } else {
+            vs[0] = (R)0.5 * Ql[5] + (R)0.5 * Qr[5];
+            vs[1] = (R)0.5 * Ql[6] + (R)0.5 * Qr[6];
+        }
+    }
+    __syncthreads();
+
+    // ---- C: divergence, B gradient, sources, RK update --------------------------
+    double part_r = 0.0, part_d = 0.0;
+    for (int t = tid; t < ncl * NN; t += NT) {
+        const int i = t % N, j = (t / N) % N, c = t / NN;
+        const int cell = c0 + c;
+        const double *met = sMet + c * ML::kSize;
+        const double J = met[ML::kJac + i + N * j];
+        const R *Fx = sF + c * S::kF + (0 * N + j) * NP * 9;  // xi-line j
+        const R *Fy = sF + c * S::kF + (1 * N + i) * NP * 9;  // eta-line i
+        const R *Vx = sV + c * S::kV + (0 * N + j) * NP * NG;
+        const R *Vy = sV + c * S::kV + (1 * N + i) * NP * NG;
+        // nablaQsp (compflux.f90:107-157) for the variables kept
+        double gB[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [Bx,By][x,y]
+        // with vismode == 0 the reference never fills nablaQs; its divB
+        // source then reads the zeros of the fresh allocation
+        if constexpr (DIAG) {
+            if (a.vismode != 1) {
+                double *go = a.grad_out + (size_t)cell * (18 * NN) + 18 * (i + N * j);
+                for (int k = 0; k < 18; k++) go[k] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < NG; g++) {
+            if (a.vismode != 1) break;
+            R ax = (R)0, ay = (R)0, bx = (R)0, by = (R)0;
+#pragma unroll
+            for (int r = 0; r < NP; r++) {
+                const R mx = Vx[r * NG + g] * opM<R>(ops, r * N + i);
+                ax = ax + mx * (R)met[ML::normal(0, j, r)];
+                ay = ay + mx * (R)met[ML::normal(0, j, r) + 1];
+            }
+#pragma unroll
+            for (int r = 0; r < NP; r++) {
+                const R my = Vy[r * NG + g] * opM<R>(ops, r * N + j);
+                bx = bx + my * (R)met[ML::normal(1, i, r)];
+                by = by + my * (R)met[ML::normal(1, i, r) + 1];
+            }
+            double gx, gy;
+            if constexpr (EX) {
+                gx = (double)(ax + bx) / J;
+                gy = (double)(ay + by) / J;
+            } else {
+                const double rJ = 1.0 / J;
+                gx = (double)(ax + bx) * rJ;
+                gy = (double)(ay + by) * rJ;
+            }
+            const int var = DIAG ? g : g + 5;
+            if (var == 5) { gB[0][0] = gx; gB[0][1] = gy; }
+            if (var == 6) { gB[1][0] = gx; gB[1][1] = gy; }
+            if constexpr (DIAG) {
+                double *go = a.grad_out + (size_t)cell * (18 * NN) + 18 * (i + N * j);
+                go[g] = gx;
+                go[9 + g] = gy;
+            }
+        }
+        const double divB = gB[0][0] + gB[1][1];
+        {
+            const double d = gB[1][0] - gB[0][1];
+            sJz[c * NN + i + N * j] = d * d;
+        }
+        // compresid.f90:12-51 divergence of the inviscid flux
+        double res[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            R dF = (R)0, dG = (R)0;
+#pragma unroll
+            for (int r = 0; r < NP; r++) {
+                dF = dF + Fx[r * 9 + k] * opM<R>(ops, r * N + i);
+                dG = dG + Fy[r * 9 + k] * opM<R>(ops, r * N + j);
+            }
+            res[k] = (double)(-(dF + dG));
+            // the viscous chain adds exactly +0.0 when mu == eta0 == 0
+            if (a.vismode == 1) res[k] = res[k] + 0.0;
+        }
+        // compresid.f90:53-78: 1/Jac, Powell 8-wave and GLM sources
+        const double *q = sQ + c * NQ + 9 * (i + N * j);
+        if constexpr (EX) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) res[k] = res[k] / J;
+        } else {
+            const double rJ = 1.0 / J;
+#pragma unroll
+            for (int k = 0; k < 9; k++) res[k] = res[k] * rJ;
+        }
+        const double Bx = q[5], By = q[6], Bz = q[7], psi = q[8];
+        double ux, uy, uz;
+        if constexpr (EX) {
+            ux = q[1] / q[0]; uy = q[2] / q[0]; uz = q[3] / q[0];
+        } else {
+            const double ri = 1.0 / q[0];
+            ux = q[1] * ri; uy = q[2] * ri; uz = q[3] * ri;
+        }
+        res[1] = res[1] - divB * Bx;
+        res[2] = res[2] - divB * By;
+        res[3] = res[3] - divB * Bz;
+        res[4] = res[4] - divB * ((ux * Bx + uy * By) + uz * Bz);
+        res[5] = res[5] - divB * ux;
+        res[6] = res[6] - divB * uy;
+        res[7] = res[7] - divB * uz;
+        res[8] = res[8] - a.alpha * psi;
+        if (a.mon_part) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) part_r += res[k] * res[k];
+            part_d += divB * divB;
+        }
+        const size_t off = (size_t)cell * NQ + 9 * (i + N * j);
+        if constexpr (DIAG) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) a.resid_out[off + k] = res[k];
+        } else {
+            double *o = a.q_out + off;
+            const double *cf = a.c;
+            switch (a.rk_kind) {
+            case kRkAxpy:
+#pragma unroll
+                for (int k = 0; k < 9; k++) o[k] = q[k] + cf[0] * res[k];
+                break;
+            case kRkTwoReg: {
+                const double *ra = a.reg_a + off;
+#pragma unroll
+                for (int k = 0; k < 9; k++) o[k] = (cf[1] * ra[k] + cf[2] * q[k]) + cf[0] * res[k];
+                if (a.resid_w) {
+#pragma unroll
+                    for (int k = 0; k < 9; k++) a.resid_w[off + k] = res[k];
+                }
+                break;
+            }
+            case kRkTwoRegT: {
+                const double *ra = a.reg_a + off;
+#pragma unroll
+                for (int k = 0; k < 9; k++) o[k] = (cf[1] * ra[k] + cf[2] * q[k]) + (cf[0] * res[k]) * cf[3];
+                break;
+            }
+            case kRkFive: {
+                const double *ra = a.reg_a + off, *rb = a.reg_b + off, *rc = a.reg_c + off, *rd = a.reg_d + off;
+#pragma unroll
+                for (int k = 0; k < 9; k++)
+                    o[k] = ((((cf[1] * ra[k] + cf[2] * rb[k]) + cf[3] * rc[k]) + cf[4] * q[k]) + cf[5] * rd[k]) +
+                           cf[0] * res[k];
+                break;
+            }
+            default: break;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- D: AV smoothness sensor (comp_artificial_viscosity, AV.f90:14-83) ------
+    if (a.artiv == 1 && a.vismode == 1) {
+        constexpr int NL = N - 1;
+        for (int t = tid; t < ncl * 2 * NL * NL; t += NT) {
+            const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
+            const double *q = sQ + c * NQ;
+            const double *jz = sJz + c * NN;
+            double acc = 0.0;
+            for (int js = 0; js < N; js++)
+#pragma unroll
+                for (int is = 0; is < N; is++) {
+                    const double x = v == 0 ? q[9 * (is + N * js)] : jz[is + N * js];
+                    acc = acc + x * ops.H[isl * N + is] * ops.H[jsl * N + js];
+                }
+            sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
+        }
+        __syncthreads();
+        for (int t = tid; t < ncl * 2; t += NT) {
+            const int v = t % 2, c = t / 2;
+            const double *q = sQ + c * NQ;
+            const double *jz = sJz + c * NN;
+            const double *lo = sLow + c * S::kLow + v * NL * NL;
+            double se = 0.0;
+            for (int js = 0; js < N; js++)
+                for (int is = 0; is < N; is++) {
+                    double hi = 0.0;
+                    for (int jsl = 0; jsl < NL; jsl++)
+#pragma unroll
+                        for (int isl = 0; isl < NL; isl++)
+                            hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
+                    const double x = v == 0 ? q[9 * (is + N * js)] : jz[is + N * js];
+                    const double d = hi - x;
+                    se = se + d * d / (x * x);
+                }
+            a.sm_ind[2 * (size_t)(c0 + c) + v] = log10(se);
+        }
+    }
+
+    // ---- reductions ------------------------------------------------------------
+    {
+        const int lane = tid & 31, wid = tid >> 5;
+        constexpr int NW = (NT + 31) / 32;
+        double em = warp_max((double)eigmax), um = warp_max((double)umax);
+        unsigned e = __reduce_or_sync(0xffffffffu, err);
+        double pr = 0.0, pd = 0.0;
+        if (a.mon_part) {
+            pr = warp_sum(part_r);
+            pd = warp_sum(part_d);
+        }
+        if (lane == 0) {
+            sRed[wid] = em;
+            sRed[32 + wid] = um;
+            sRed[64 + wid] = pr;
+            sRed[96 + wid] = pd;
+            if (e) atomicOr(a.err_flags, e);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double m0 = 0.0, m1 = 0.0, s0 = 0.0, s1 = 0.0;
+            for (int w = 0; w < NW; w++) {
+                m0 = sRed[w] > m0 ? sRed[w] : m0;
+                m1 = sRed[32 + w] > m1 ? sRed[32 + w] : m1;
+                s0 += sRed[64 + w];
+                s1 += sRed[96 + w];
+            }
+            atomic_max_nonneg(&a.maxima[2 * a.slot_w], m0);
+            atomic_max_nonneg(&a.maxima[2 * a.slot_w + 1], m1);
+            if (blockIdx.x == 0) {  // carry the previous stages' maxima forward
+                atomic_max_nonneg(&a.maxima[2 * a.slot_w], eig_r);
+                atomic_max_nonneg(&a.maxima[2 * a.slot_w + 1], um_r);
+            }
+            if (a.mon_part) {
+                a.mon_part[2 * blockIdx.x] = s0;
+                a.mon_part[2 * blockIdx.x + 1] = s1;
+            }
+        }
+    }
+}
+
+template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
+{
+    using S = Smem<N, R, DIAG>;
+    size_t d = (size_t)CPB * (S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
+    size_t r = (size_t)CPB * (S::kF + S::kV + (sizeof(R) == sizeof(double) ? 0 : S::NQ));
+    return d * sizeof(double) + r * sizeof(R);
+}
+
+}  // namespace sddc

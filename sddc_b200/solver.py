@@ -1,0 +1,218 @@
+"""The drop-in, driven from Python through its C ABI (include/sddc.h).
+
+``Solver`` mirrors what the reference's Fortran host does around the hot
+path: it passes the set-up tables once (``sddc_set_tables``), the state
+(``sddc_set_state``, the restart route of initsetup.f90:154-162), then calls
+``compresid`` or ``rk_s5p3`` (RK_S5P3, iterations.f90:158-213) and reads
+results back.  ``iterations`` replays the reference's time loop with its
+residual monitor (iterations.f90:19-83).
+
+There is no CPU path: a missing or unloadable ``libsddc_b200.so`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _native
+from ._native import ptr
+
+_I = ctypes.c_int
+_D = ctypes.c_double
+_PI = ctypes.POINTER(ctypes.c_int)
+_PD = ctypes.POINTER(ctypes.c_double)
+
+FP64_EXACT, FP64, MIXED = 0, 1, 2
+PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "mixed": MIXED}
+
+OK, EINVAL, ECUDA, ESTATE, ENUMERIC, ENOMEM = 0, -1, -2, -3, -4, -5
+
+EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables", "sddc_set_state",
+            "sddc_compresid", "sddc_rk_step", "sddc_get_state", "sddc_monitor", "sddc_get_maxima",
+            "sddc_state_device_ptr", "sddc_get_stream")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("N", _I), ("ncell", _I), ("ncellglob", _I), ("vismode", _I), ("artiv", _I), ("k_stage", _I),
+                ("precision", _I), ("cells_per_cta", _I), ("mu", _D), ("eta0", _D), ("dxcycl", _D),
+                ("dycycl", _D), ("rinf", _D), ("pinf", _D), ("uinf", _D), ("vinf", _D), ("bxinf", _D),
+                ("byinf", _D)]
+
+
+class SddcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sddc error {code}: {msg}")
+        self.code = code
+
+
+class NumericalFault(SddcError):
+    """The device saw a non-positive density or a non-finite wave speed."""
+
+
+def lib():
+    L = _native.load(_native.GPU_LIB)
+    if not getattr(L, "_sddc_typed", False):
+        L.sddc_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Params)]
+        L.sddc_destroy.argtypes = [ctypes.c_void_p]
+        L.sddc_destroy.restype = None
+        L.sddc_last_error.argtypes = [ctypes.c_void_p]
+        L.sddc_last_error.restype = ctypes.c_char_p
+        L.sddc_set_tables.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD, _PI, _I] + [_PI, _I] * 7
+        L.sddc_set_state.argtypes = [ctypes.c_void_p, _PD, _D, _D, _D]
+        L.sddc_compresid.argtypes = [ctypes.c_void_p]
+        L.sddc_rk_step.argtypes = [ctypes.c_void_p, _D, _I]
+        L.sddc_get_state.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD]
+        L.sddc_monitor.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD]
+        L.sddc_get_maxima.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD]
+        L.sddc_state_device_ptr.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.sddc_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L._sddc_typed = True
+    return L
+
+
+class Solver:
+    """One case on the current GPU."""
+
+    def __init__(self, tables, physics, precision="fp64", k_stage: int = 3, cells_per_cta: int = 0,
+                 ncellglob: int | None = None):
+        self.N = tables.N
+        self.ncell = tables.ncell
+        self.tables = tables
+        self.physics = physics
+        self.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self.k_stage = k_stage
+        p = Params(N=tables.N, ncell=tables.ncell, ncellglob=ncellglob or tables.ncell, vismode=physics.vismode,
+                   artiv=physics.artiv, k_stage=k_stage, precision=self.precision, cells_per_cta=cells_per_cta,
+                   mu=physics.mu, eta0=physics.eta0, dxcycl=physics.dxcycl, dycycl=physics.dycycl,
+                   rinf=physics.rinf, pinf=physics.pinf, uinf=physics.uinf, vinf=physics.vinf,
+                   bxinf=physics.bxinf, byinf=physics.byinf)
+        self._L = lib()
+        self._h = ctypes.c_void_p()
+        rc = self._L.sddc_create(ctypes.byref(self._h), ctypes.byref(p))
+        if rc != OK:
+            msg = self._L.sddc_last_error(self._h).decode() if self._h else "sddc_create failed"
+            self.close()
+            raise SddcError(rc, msg)
+        t = tables
+        keep = []
+
+        def ia(a):
+            a = np.asfortranarray(a, dtype=np.int32)
+            keep.append(a)
+            return ptr(a, _I)
+
+        def da(a):
+            a = np.asfortranarray(a, dtype=np.float64)
+            keep.append(a)
+            return ptr(a)
+
+        self._check(self._L.sddc_set_tables(
+            self._h, da(t.Lmat), da(t.Mmat), da(t.S1), da(t.S2), da(t.Jac), ia(t.IF2C), t.nface,
+            ia(t.ibfinter), len(t.ibfinter), ia(t.ibfinl), len(t.ibfinl), ia(t.ibfout), len(t.ibfout),
+            ia(t.ibfwal), len(t.ibfwal), ia(t.ibfsymp), len(t.ibfsymp), ia(t.ibfree), len(t.ibfree),
+            ia(t.cyc2fpair), int(t.cyc2fpair.shape[0])))
+
+    # -- plumbing ----------------------------------------------------------
+    def _check(self, rc):
+        if rc == OK:
+            return
+        msg = self._L.sddc_last_error(self._h).decode()
+        if rc == ENUMERIC:
+            raise NumericalFault(rc, msg)
+        raise SddcError(rc, msg)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._L.sddc_destroy(h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- the reference-facing calls -----------------------------------------
+    def set_state(self, Q, ctime=0.0, eigvmax=0.0, umax=0.0):
+        Q = np.asfortranarray(Q, dtype=np.float64)
+        assert Q.shape == (9, self.N, self.N, self.ncell)
+        self._check(self._L.sddc_set_state(self._h, ptr(Q), ctime, eigvmax, umax))
+
+    def compresid(self):
+        self._check(self._L.sddc_compresid(self._h))
+
+    def rk_s5p3(self, dt, nsteps=1):
+        """nsteps time steps with the context's scheme (k_stage 3 or 5)."""
+        self._check(self._L.sddc_rk_step(self._h, float(dt), int(nsteps)))
+
+    step = rk_s5p3
+
+    def state(self, resid=False, nablaQs=False, muAV=False, sm_ind=False, out=None):
+        N, nc = self.N, self.ncell
+        Q = out if out is not None else np.zeros((9, N, N, nc), order="F")
+        R = np.zeros((9, N, N, nc), order="F") if resid else None
+        G = np.zeros((9, 2, N, N, nc), order="F") if nablaQs else None
+        M = np.zeros((2, nc), order="F") if muAV else None
+        S = np.zeros((2, nc), order="F") if sm_ind else None
+        self._check(self._L.sddc_get_state(self._h, ptr(Q), ptr(R), ptr(G), ptr(M), ptr(S)))
+        d = dict(Q=Q)
+        for k, v in (("resid", R), ("nablaQs", G), ("muAV", M), ("sm_ind", S)):
+            if v is not None:
+                d[k] = v
+        return d
+
+    def monitor(self):
+        v = [_D() for _ in range(4)]
+        self._check(self._L.sddc_monitor(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(residsum=v[0].value, divbsum=v[1].value, mass=v[2].value, energy=v[3].value)
+
+    def maxima(self):
+        v = [_D() for _ in range(4)]
+        self._check(self._L.sddc_get_maxima(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(eigvmax=v[0].value, umax=v[1].value, c_h=v[2].value, ctime=v[3].value)
+
+    def device_state_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self._L.sddc_state_device_ptr(self._h, ctypes.byref(p)))
+        return p.value
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t of the context (for CUDA events around its work)."""
+        p = ctypes.c_void_p()
+        self._check(self._L.sddc_get_stream(self._h, ctypes.byref(p)))
+        return p.value
+
+    # -- the reference's time loop -------------------------------------------
+    def iterations(self, dt, maxiter, resid_out=None, iter0=0, ncellglob=None):
+        """The loop of iterations.f90:19-83 with its residual monitor every
+        10 iterations (mod(iter,10)==1); returns the monitor rows
+        (iter, ctime, RESIDNORM, divB)."""
+        rows = []
+        ncg = ncellglob or self.ncell
+        it = iter0
+        if resid_out:
+            with open(resid_out, "w") as f:
+                f.write(" ITER    ctime     RESIDNORM   divB\n")
+        while True:
+            it += 1
+            self.rk_s5p3(dt, 1)
+            if it % 10 == 1:
+                m = self.monitor()
+                rn = math.sqrt(m["residsum"] / (ncg * self.N * self.N * 9))
+                db = math.sqrt(m["divbsum"] / (ncg * self.N * self.N))
+                rows.append((it, self.maxima()["ctime"], rn, db))
+                if resid_out:
+                    with open(resid_out, "a") as f:
+                        f.write(f" {it} {rows[-1][1]!r} {rn!r} {db!r}\n")
+            if it >= maxiter:
+                break
+        return rows
