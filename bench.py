@@ -120,10 +120,17 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+TILES = {}
+
+
 def time_form(torch, solver_mod, t, ph, Q0, dt, precision, steps, warmup):
     """Device time of `steps` RK3 steps (state resident), CUDA events on the
-    context's stream."""
-    s = solver_mod.Solver(t, ph, precision=precision)
+    context's stream; the tile is picked by the autotuner first (untimed)."""
+    from sddc_b200 import autotune
+
+    cpb, times = autotune.tune(t, ph, Q0, dt, precision)
+    TILES[precision] = {"cells_per_cta": cpb, "tuning_s_per_step": times}
+    s = solver_mod.Solver(t, ph, precision=precision, cells_per_cta=cpb)
     s.set_state(Q0)
     s.rk_s5p3(dt, warmup)
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -162,6 +169,16 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    if args.only:
+        # one form only, no e2e or baselines: the command profiled under ncu
+        s, ms = time_form(torch, solver_mod, t, ph, Q0, dt, args.only, steps, warm)
+        s.close()
+        if rank == 0:
+            print(json.dumps({"profile_run": args.only, "steps": steps, "ms_per_step": ms / steps,
+                              "dof_stage_per_s": dof * 5 * steps / (ms / 1e3)}))
+        if dist:
+            dist.destroy_process_group()
+        return
     results = {}
     states = {}
     try:
@@ -255,6 +272,7 @@ def run_ours(args):
             "physics": f"ideal MHD gamma=5/3, Ms={MS}, MA={MA}, seeded U(+-1e-6) noise",
             "l2": "inputs larger than L2 (236 MB per state register)",
             "parallelism": "replicas" if world > 1 else "single GPU",
+            "tiles": TILES,
         },
         "fp64": {"value": val["fp64"], "ms_per_step": results["fp64"] / steps},
         "fp64_exact": {"value": val["fp64_exact"], "ms_per_step": results["fp64_exact"] / steps},
@@ -334,6 +352,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["mixed", "fp64", "fp64_exact"], default=None,
+                    help="time one form only (the command used for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

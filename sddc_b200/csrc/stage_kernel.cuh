@@ -143,10 +143,30 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
+{
+    using S = Smem<N, R, DIAG>;
+    size_t d = (size_t)CPB * (S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
+    size_t r = (size_t)CPB * (S::kF + S::kV + (sizeof(R) == sizeof(double) ? 0 : S::NQ));
+    return d * sizeof(double) + r * sizeof(R);
+}
+
+// CTAs per SM the kernel is compiled for: as many as the 228 KB of shared
+// memory per SM hold (1 KB per CTA is the driver's), but no fewer than 96
+// registers per thread
+template <int N, int CPB, typename R, bool DIAG> constexpr int stage_min_blocks()
+{
+    int b = (int)((228 * 1024) / (stage_smem_bytes<N, CPB, R, DIAG>() + 1024));
+    b = b < 1 ? 1 : (b > 8 ? 8 : b);
+    while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < 96) b--;
+    return b;
+}
+
 // EXACT instantiations are compiled without FMA contraction (-fmad=false) in
 // their own translation unit; they reproduce the reference's FP64 rounding.
 template <int N, int CPB, typename R, bool DIAG, bool EXACT>
-__global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const StageArgs a, const Ops ops)
+__global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
+    stage_kernel(const StageArgs a, const Ops ops)
 {
     constexpr bool EX = EXACT && (sizeof(R) == sizeof(double));
     using S = Smem<N, R, DIAG>;
@@ -245,10 +265,11 @@ __global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const Stag
         const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
         const int kind = rec.y & 0xff;
         const double *onrm = sMet + c * ML::kSize + ML::normal(fam, line, r);
-        const R *Ql, *Qr;
         R n0, n1;
         int sign_l, sign_r;
-        if (kind == kFaceLeft || kind == kFaceRight) {
+        const bool pair = kind == kFaceLeft || kind == kFaceRight;
+        const bool own_right = kind == kFaceRight;
+        if (pair) {
             // partner point N-nfp+1 on the partner's local face
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
             int pfam, pline, pr;
@@ -262,13 +283,11 @@ __global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const Stag
                 for (int s = 0; s < N; s++) acc = acc + (R)__ldg(qp + k + stride * s) * opL<R>(ops, pr * N + s);
                 other[k] = acc;
             }
-            if (kind == kFaceLeft) {
-                Ql = own; Qr = other;
+            if (!own_right) {
                 n0 = (R)onrm[0]; n1 = (R)onrm[1];
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = pr == N ? -1 : 1;
             } else {
-                Ql = other; Qr = own;
                 const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
                 n0 = (R)__ldg(pn);
                 n1 = (R)__ldg(pn + 1);
@@ -280,16 +299,22 @@ __global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const Stag
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
             bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.fs, other);
-            Ql = own; Qr = other;
+        }
+        // left and right states by element-wise selects (arrays picked
+        // through a pointer would live in local memory)
+        R Ql[9], Qr[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            Ql[k] = own_right ? other[k] : own[k];
+            Qr[k] = own_right ? own[k] : other[k];
         }
         if (!(Ql[0] > (R)0) || !(Qr[0] > (R)0)) err |= kErrNonPositiveDensity;
         R eig_face;
         rusanov<R, EX>(Ql, Qr, Fl, Fr, n0, n1, sign_l, sign_r, c_h, eig_face, umax);
         if (!(Abs<R>(eig_face) < (R)INFINITY)) err |= kErrNonFiniteWaveSpeed;
         if (eig_face > eigmax) eigmax = eig_face;
-        const R *fo = (kind == kFaceRight) ? Fr : Fl;
 #pragma unroll
-        for (int k = 0; k < 9; k++) slot[k] = fo[k];
+        for (int k = 0; k < 9; k++) slot[k] = own_right ? Fr[k] : Fl[k];
         R *vs = sV + c * S::kV + ((fam * N + line) * NP + r) * NG;
         if constexpr (DIAG) {
 #pragma unroll
@@ -465,24 +490,30 @@ __global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const Stag
             sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
         }
         __syncthreads();
-        for (int t = tid; t < ncl * 2; t += NT) {
-            const int v = t % 2, c = t / 2;
-            const double *q = sQ + c * NQ;
-            const double *jz = sJz + c * NN;
+        // projection back to the solution points and the terms of the sensor
+        // sum, one thread per (cell, variable, point); the flux buffer is
+        // free after phase C and holds the terms
+        double *sTerm = reinterpret_cast<double *>(sF);  // [CPB][2][NN]
+        for (int t = tid; t < ncl * 2 * NN; t += NT) {
+            const int is = t % N, js = (t / N) % N, v = (t / NN) % 2, c = t / (2 * NN);
             const double *lo = sLow + c * S::kLow + v * NL * NL;
-            double se = 0.0;
-            for (int js = 0; js < N; js++)
-                for (int is = 0; is < N; is++) {
-                    double hi = 0.0;
-                    for (int jsl = 0; jsl < NL; jsl++)
+            double hi = 0.0;
+            for (int jsl = 0; jsl < NL; jsl++)
 #pragma unroll
-                        for (int isl = 0; isl < NL; isl++)
-                            hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
-                    const double x = v == 0 ? q[9 * (is + N * js)] : jz[is + N * js];
-                    const double d = hi - x;
-                    se = se + d * d / (x * x);
-                }
-            a.sm_ind[2 * (size_t)(c0 + c) + v] = log10(se);
+                for (int isl = 0; isl < NL; isl++)
+                    hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
+            const double x = v == 0 ? sQ[c * NQ + 9 * (is + N * js)] : sJz[c * NN + is + N * js];
+            const double d = hi - x;
+            sTerm[(c * 2 + v) * NN + is + N * js] = d * d / (x * x);
+        }
+        __syncthreads();
+        // the sum in the reference's (js, is) order
+        for (int t = tid; t < ncl * 2; t += NT) {
+            const double *tm = sTerm + t * NN;
+            double se = 0.0;
+#pragma unroll
+            for (int k = 0; k < NN; k++) se = se + tm[k];
+            a.sm_ind[2 * (size_t)c0 + t] = log10(se);
         }
     }
 
@@ -525,14 +556,6 @@ __global__ void __launch_bounds__(stage_threads(N, CPB)) stage_kernel(const Stag
             }
         }
     }
-}
-
-template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
-{
-    using S = Smem<N, R, DIAG>;
-    size_t d = (size_t)CPB * (S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
-    size_t r = (size_t)CPB * (S::kF + S::kV + (sizeof(R) == sizeof(double) ? 0 : S::NQ));
-    return d * sizeof(double) + r * sizeof(R);
 }
 
 }  // namespace sddc
