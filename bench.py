@@ -121,6 +121,7 @@ class Clocks:
 
 
 TILES = {}
+FIXED_TILE = 0
 
 
 def time_form(torch, solver_mod, t, ph, Q0, dt, precision, steps, warmup):
@@ -128,7 +129,10 @@ def time_form(torch, solver_mod, t, ph, Q0, dt, precision, steps, warmup):
     context's stream; the tile is picked by the autotuner first (untimed)."""
     from sddc_b200 import autotune
 
-    cpb, times = autotune.tune(t, ph, Q0, dt, precision)
+    if FIXED_TILE:
+        cpb, times = FIXED_TILE, None
+    else:
+        cpb, times = autotune.tune(t, ph, Q0, dt, precision)
     TILES[precision] = {"cells_per_cta": cpb, "tuning_s_per_step": times}
     s = solver_mod.Solver(t, ph, precision=precision, cells_per_cta=cpb)
     s.set_state(Q0)
@@ -204,8 +208,8 @@ def run_ours(args):
     barrier()
     # end-to-end through the C ABI with host buffers, every step:
     # state host->device, one RK3 step, state and monitor device->host
-    s = solver_mod.Solver(t, ph, precision="mixed")
-    q_host = torch.empty(Q0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(Q0.shape, order="F")
+    s = solver_mod.Solver(t, ph, precision="mixed", cells_per_cta=TILES["mixed"]["cells_per_cta"])
+    q_host =torch.empty(Q0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(Q0.shape, order="F")
     q_host[...] = Q0
     out_host = torch.empty(Q0.size, dtype=torch.float64, pin_memory=True).numpy().reshape(Q0.shape, order="F")
     s.set_state(q_host)
@@ -354,7 +358,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["mixed", "fp64", "fp64_exact"], default=None,
                     help="time one form only (the command used for ncu captures)")
+    ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8, 16],
+                    help="cells per CTA; 0 lets the autotuner choose")
     args = ap.parse_args()
+    global FIXED_TILE
+    FIXED_TILE = args.tile
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

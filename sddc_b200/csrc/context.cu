@@ -23,6 +23,9 @@ namespace sddc {
 cudaError_t launch_stage_exact(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
 cudaError_t launch_stage_fp64(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
 cudaError_t launch_stage_mixed(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
+cudaError_t launch_trace_exact(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
+cudaError_t launch_trace_fp64(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
+cudaError_t launch_trace_mixed(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
 }  // namespace sddc
 
 using namespace sddc;
@@ -172,6 +175,8 @@ struct sddc_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     double *reg[kRegs] = {};
+    void *trace[kRegs] = {};  // face traces of each register (float in the mixed form)
+    size_t trace_bytes = 0;
     double *met = nullptr;
     int2 *faces = nullptr;
     double *maxima = nullptr;  // [kSlots][2]
@@ -183,6 +188,7 @@ struct sddc_ctx {
     int slot = 0;  // slot holding the running maxima after the last evaluation
     int mon_nblk = 0;  // CTAs of the last launch that wrote monitor partials
     bool tables = false, state = false;
+    bool traces_stale = true;  // trace[0] does not match reg[0] yet
     double ctime = 0.0;
     cudaGraphExec_t graph[kSlots] = {};
     double graph_dt[kSlots] = {};
@@ -215,6 +221,7 @@ static void free_all(sddc_ctx *ctx)
             g = nullptr;
         }
     for (auto &r : ctx->reg) cudaFree(r), r = nullptr;
+    for (auto &t : ctx->trace) cudaFree(t), t = nullptr;
     void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
                     ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags};
     for (void *b : bufs) cudaFree(b);
@@ -271,8 +278,11 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     const int nreg = p->k_stage == 5 ? 6 : 4;
     int rc;
-    for (int r = 0; r < nreg; r++)
+    ctx->trace_bytes = (size_t)p->ncell * 4 * p->N * 9 * (p->precision == SDDC_MIXED ? sizeof(float) : sizeof(double));
+    for (int r = 0; r < nreg; r++) {
         if ((rc = alloc(ctx, (void **)&ctx->reg[r], ctx->nq * sizeof(double), "state register"))) return rc;
+        if ((rc = alloc(ctx, &ctx->trace[r], ctx->trace_bytes, "face traces"))) return rc;
+    }
     const size_t nc = p->ncell;
     const int diag_grid = (p->ncell + 7) / 8;
     const int mon_blocks = std::max(ctx->grid, diag_grid);
@@ -397,6 +407,22 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
     CK(cudaMemcpyAsync(ctx->faces, fr.data(), fr.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->tables = true;
+    ctx->traces_stale = true;
+    return SDDC_OK;
+}
+
+// face traces of the current state (register 0), computed by the form's own
+// translation unit so they round exactly as its stage kernel's
+static int refresh_traces(sddc_ctx *ctx)
+{
+    cudaError_t e;
+    switch (ctx->p.precision) {
+    case SDDC_FP64_EXACT: e = launch_trace_exact(ctx->N, ctx->ncell, ctx->reg[0], ctx->trace[0], ctx->ops, ctx->stream); break;
+    case SDDC_FP64: e = launch_trace_fp64(ctx->N, ctx->ncell, ctx->reg[0], ctx->trace[0], ctx->ops, ctx->stream); break;
+    default: e = launch_trace_mixed(ctx->N, ctx->ncell, ctx->reg[0], ctx->trace[0], ctx->ops, ctx->stream); break;
+    }
+    if (e != cudaSuccess) return cuda_err(ctx, e, "trace kernel");
+    ctx->traces_stale = false;
     return SDDC_OK;
 }
 
@@ -410,6 +436,12 @@ extern "C" int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, doub
         mx[2 * s + 1] = umax;
     }
     CK(cudaMemcpyAsync(ctx->maxima, mx, sizeof(mx), cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->tables) {
+        int rc = refresh_traces(ctx);
+        if (rc) return rc;
+    } else {
+        ctx->traces_stale = true;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->ctime = ctime;
     ctx->slot = 0;
@@ -447,6 +479,7 @@ static int ready(sddc_ctx *ctx)
     if (!ctx) return SDDC_EINVAL;
     if (!ctx->tables) return set_err(ctx, SDDC_ESTATE, "tables not set (call sddc_set_tables)");
     if (!ctx->state) return set_err(ctx, SDDC_ESTATE, "state not set (call sddc_set_state)");
+    if (ctx->traces_stale) return refresh_traces(ctx);
     return SDDC_OK;
 }
 
@@ -481,6 +514,7 @@ extern "C" int sddc_compresid(sddc_ctx *ctx)
     StageArgs a = base_args(ctx);
     a.rk_kind = kRkNone;
     a.q_in = ctx->reg[0];
+    a.t_in = ctx->trace[0];
     a.slot_r = ctx->slot;
     a.slot_w = (ctx->slot + 1) % kSlots;
     a.resid_out = ctx->resid;
@@ -521,6 +555,8 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
         a.rk_kind = st[k].kind;
         a.q_in = P[st[k].in];
         a.q_out = P[st[k].out];
+        a.t_in = ctx->trace[st[k].in];
+        a.t_out = ctx->trace[st[k].out];
         a.reg_a = st[k].ra >= 0 ? P[st[k].ra] : nullptr;
         a.reg_b = st[k].rb >= 0 ? P[st[k].rb] : nullptr;
         a.reg_c = st[k].rc >= 0 ? P[st[k].rc] : nullptr;

@@ -3,4 +3,5 @@
 #define SDDC_R double
 #define SDDC_EXACT_FORM true
 #define SDDC_LAUNCH launch_stage_exact
+#define SDDC_TRACE launch_trace_exact
 #include "stage_launch.inc"

@@ -12,15 +12,17 @@
 //      flux points (one thread per cell x family x line x variable);
 //   B1 physical flux at the interior flux points (thread per point);
 //   B2 Rusanov flux at the 4N face points of each cell (thread per point).
-//      The neighbour's trace is interpolated from the neighbour's state in
-//      global memory (served by L2; neighbours are a few cells away in
-//      memory).  Each shared face is evaluated by both of its cells, each
-//      with the reference's left/right assignment, so both get the value
-//      the reference scatters to them;
+//      The neighbour's trace at the face (9 contiguous values) comes from
+//      the trace buffer that the stage producing the input published.  Each
+//      shared face is evaluated by both of its cells, each with the
+//      reference's left/right assignment, so both get the value the
+//      reference scatters to them;
 //   C  divergence of the flux, gradient of (Bx, By) from the face-averaged
-//      flux-point states, Powell and GLM sources and the RK update (thread
-//      per solution point);
-//   D  the AV smoothness sensor per cell.
+//      flux-point states, Powell and GLM sources (thread per solution point);
+//   D  the AV smoothness sensor per cell;
+//   E  the RK stage update, element-wise over the CTA's contiguous slice of
+//      the state (coalesced loads of the RK registers and stores);
+//   F  the face traces of the output state, published for the next stage.
 // Running maxima of the wave speed and of the velocity (the c_h input of
 // the next stage) go through atomicMax on five rotating slots, so that
 // launches need no host synchronisation.
@@ -69,6 +71,8 @@ struct StageArgs {
     Freestream fs;
     const double *__restrict__ q_in;   // (9,N,N,NCELL), never written during the stage
     double *q_out;                     // RK output (may be reg_a: FiveStageRk stage 5)
+    const void *__restrict__ t_in;     // face traces of q_in, R[NCELL][4][N][9]
+    void *t_out;                       // face traces of q_out (null: not produced)
     const double *reg_a;               // RK registers read by this stage
     const double *reg_b;
     const double *reg_c;
@@ -146,7 +150,7 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    size_t d = (size_t)CPB * (S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
+    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
     size_t r = (size_t)CPB * (S::kF + S::kV + (sizeof(R) == sizeof(double) ? 0 : S::NQ));
     return d * sizeof(double) + r * sizeof(R);
 }
@@ -181,7 +185,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *sJz = sMet + CPB * ML::kSize;                        // [CPB][NN]  Jz^2 for the sensor
     double *sLow = sJz + CPB * NN;                               // [CPB][kLow]
     double *sRed = sLow + CPB * S::kLow;                         // [4][32] block reductions
-    R *sF = reinterpret_cast<R *>(sRed + 4 * 32);                // [CPB][2][N][NP][9]
+    double *sRes = sRed + 4 * 32;                                // [CPB][NQ] residual
+    R *sF = reinterpret_cast<R *>(sRes + CPB * NQ);              // [CPB][2][N][NP][9]
     R *sV = sF + CPB * S::kF;                                    // [CPB][2][N][NP][NG]
     R *sQr = sV + CPB * S::kV;                                   // [CPB][NQ] (float form only)
 
@@ -270,19 +275,14 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         const bool pair = kind == kFaceLeft || kind == kFaceRight;
         const bool own_right = kind == kFaceRight;
         if (pair) {
-            // partner point N-nfp+1 on the partner's local face
+            // partner point N-nfp+1 on the partner's local face; its trace was
+            // published by the stage that produced q_in
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
             int pfam, pline, pr;
             face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
-            const double *qp = a.q_in + (size_t)pc * NQ + (pfam == 0 ? 9 * N * pline : 9 * pline);
-            const int stride = pfam == 0 ? 9 : 9 * N;
+            const R *tp = reinterpret_cast<const R *>(a.t_in) + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 9;
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
-                R acc = (R)0;
-#pragma unroll
-                for (int s = 0; s < N; s++) acc = acc + (R)__ldg(qp + k + stride * s) * opL<R>(ops, pr * N + s);
-                other[k] = acc;
-            }
+            for (int k = 0; k < 9; k++) other[k] = tp[k];
             if (!own_right) {
                 n0 = (R)onrm[0]; n1 = (R)onrm[1];
                 sign_l = r == 0 ? -1 : 1;
@@ -431,50 +431,16 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             for (int k = 0; k < 9; k++) part_r += res[k] * res[k];
             part_d += divB * divB;
         }
-        const size_t off = (size_t)cell * NQ + 9 * (i + N * j);
-        if constexpr (DIAG) {
+        // stage the residual; the RK update runs element-wise below
+        double *rs = sRes + c * NQ + 9 * (i + N * j);
 #pragma unroll
-            for (int k = 0; k < 9; k++) a.resid_out[off + k] = res[k];
-        } else {
-            double *o = a.q_out + off;
-            const double *cf = a.c;
-            switch (a.rk_kind) {
-            case kRkAxpy:
-#pragma unroll
-                for (int k = 0; k < 9; k++) o[k] = q[k] + cf[0] * res[k];
-                break;
-            case kRkTwoReg: {
-                const double *ra = a.reg_a + off;
-#pragma unroll
-                for (int k = 0; k < 9; k++) o[k] = (cf[1] * ra[k] + cf[2] * q[k]) + cf[0] * res[k];
-                if (a.resid_w) {
-#pragma unroll
-                    for (int k = 0; k < 9; k++) a.resid_w[off + k] = res[k];
-                }
-                break;
-            }
-            case kRkTwoRegT: {
-                const double *ra = a.reg_a + off;
-#pragma unroll
-                for (int k = 0; k < 9; k++) o[k] = (cf[1] * ra[k] + cf[2] * q[k]) + (cf[0] * res[k]) * cf[3];
-                break;
-            }
-            case kRkFive: {
-                const double *ra = a.reg_a + off, *rb = a.reg_b + off, *rc = a.reg_c + off, *rd = a.reg_d + off;
-#pragma unroll
-                for (int k = 0; k < 9; k++)
-                    o[k] = ((((cf[1] * ra[k] + cf[2] * rb[k]) + cf[3] * rc[k]) + cf[4] * q[k]) + cf[5] * rd[k]) +
-                           cf[0] * res[k];
-                break;
-            }
-            default: break;
-            }
-        }
+        for (int k = 0; k < 9; k++) rs[k] = res[k];
     }
     __syncthreads();
 
     // ---- D: AV smoothness sensor (comp_artificial_viscosity, AV.f90:14-83) ------
-    if (a.artiv == 1 && a.vismode == 1) {
+    const bool av = a.artiv == 1 && a.vismode == 1;
+    if (av) {
         constexpr int NL = N - 1;
         for (int t = tid; t < ncl * 2 * NL * NL; t += NT) {
             const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
@@ -491,9 +457,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         }
         __syncthreads();
         // projection back to the solution points and the terms of the sensor
-        // sum, one thread per (cell, variable, point); the flux buffer is
-        // free after phase C and holds the terms
-        double *sTerm = reinterpret_cast<double *>(sF);  // [CPB][2][NN]
+        // sum, one thread per (cell, variable, point); the face-state buffer
+        // is free after phase C and holds the terms
+        double *sTerm = reinterpret_cast<double *>(sV);  // [CPB][2][NN]
         for (int t = tid; t < ncl * 2 * NN; t += NT) {
             const int is = t % N, js = (t / N) % N, v = (t / NN) % 2, c = t / (2 * NN);
             const double *lo = sLow + c * S::kLow + v * NL * NL;
@@ -514,6 +480,53 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int k = 0; k < NN; k++) se = se + tm[k];
             a.sm_ind[2 * (size_t)c0 + t] = log10(se);
+        }
+    }
+
+    // ---- E: RK stage update, element-wise and coalesced (iterations.f90) -------
+    {
+        const size_t g0 = (size_t)c0 * NQ;
+        const int n = ncl * NQ;
+        if constexpr (DIAG) {
+            for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sRes[e];
+        } else {
+            const double *cf = a.c;
+            for (int e = tid; e < n; e += NT) {
+                const size_t g = g0 + e;
+                const double q = sQ[e], r = sRes[e];
+                double o;
+                switch (a.rk_kind) {
+                case kRkAxpy: o = q + cf[0] * r; break;
+                case kRkTwoReg: o = (cf[1] * a.reg_a[g] + cf[2] * q) + cf[0] * r; break;
+                case kRkTwoRegT: o = (cf[1] * a.reg_a[g] + cf[2] * q) + (cf[0] * r) * cf[3]; break;
+                default:
+                    o = ((((cf[1] * a.reg_a[g] + cf[2] * a.reg_b[g]) + cf[3] * a.reg_c[g]) + cf[4] * q) +
+                         cf[5] * a.reg_d[g]) + cf[0] * r;
+                    break;
+                }
+                a.q_out[g] = o;
+                if (a.resid_w) a.resid_w[g] = r;
+                sQ[e] = o;  // the sensor read sQ before the barrier above
+            }
+        }
+    }
+
+    // ---- F: face traces of the output state for the next stage's neighbours ---
+    if (!DIAG && a.t_out) {
+        __syncthreads();
+        R *to = reinterpret_cast<R *>(a.t_out) + (size_t)c0 * 4 * N * 9;
+        for (int t = tid; t < ncl * 4 * N * 9; t += NT) {
+            const int k = t % 9, nfp = 1 + (t / 9) % N, lf = 1 + (t / (9 * N)) % 4, c = t / (36 * N);
+            int fam, line, r;
+            face_point<N>(lf, nfp, fam, line, r);
+            const double *q = sQ + c * NQ;
+            R acc = (R)0;
+#pragma unroll
+            for (int s = 0; s < N; s++) {
+                const double x = fam == 0 ? q[k + 9 * (s + N * line)] : q[k + 9 * (line + N * s)];
+                acc = acc + (R)x * opL<R>(ops, r * N + s);
+            }
+            to[t] = acc;
         }
     }
 
@@ -555,6 +568,29 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 a.mon_part[2 * blockIdx.x + 1] = s1;
             }
         }
+    }
+}
+
+// Face traces of a state: T[cell][lf][nfp][k] = sum_s Q(k, line points) *
+// L(r, s) at the flux point of local face lf, face point nfp -- the same
+// interpolation, in the same order and type, as phase A and phase F.
+template <int N, typename R, bool EXACT>  // EXACT: compiled with -fmad=false, like phase A
+__global__ void trace_kernel(int ncell, const double *__restrict__ q, R *__restrict__ t, const Ops ops)
+{
+    const size_t n = (size_t)ncell * 4 * N * 9;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(e % 9), nfp = 1 + (int)((e / 9) % N), lf = 1 + (int)((e / (9 * N)) % 4);
+        const size_t c = e / (36 * N);
+        int fam, line, r;
+        face_point<N>(lf, nfp, fam, line, r);
+        const double *qc = q + c * (9 * N * N);
+        R acc = (R)0;
+#pragma unroll
+        for (int s = 0; s < N; s++) {
+            const double x = fam == 0 ? qc[k + 9 * (s + N * line)] : qc[k + 9 * (line + N * s)];
+            acc = acc + (R)x * opL<R>(ops, r * N + s);
+        }
+        t[e] = acc;
     }
 }
 

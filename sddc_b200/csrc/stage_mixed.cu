@@ -3,4 +3,5 @@
 #define SDDC_R float
 #define SDDC_EXACT_FORM false
 #define SDDC_LAUNCH launch_stage_mixed
+#define SDDC_TRACE launch_trace_mixed
 #include "stage_launch.inc"
