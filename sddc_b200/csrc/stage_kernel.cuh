@@ -150,8 +150,8 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kSize + N * N + S::kLow) + 4 * 32;
-    size_t r = (size_t)CPB * (S::kF + S::kV + (sizeof(R) == sizeof(double) ? 0 : S::NQ));
+    size_t d = (size_t)CPB * (2 * S::NQ + 2 * N * N + S::kLow) + 4 * 32;
+    size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam);
     return d * sizeof(double) + r * sizeof(R);
 }
 
@@ -180,15 +180,16 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     constexpr int NN = N * N;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NM = 2 * ML::kFam;  // normals per cell
     double *sQ = reinterpret_cast<double *>(smem_raw);          // [CPB][NQ]
-    double *sMet = sQ + CPB * NQ;                                // [CPB][ML::kSize]
-    double *sJz = sMet + CPB * ML::kSize;                        // [CPB][NN]  Jz^2 for the sensor
+    double *sJac = sQ + CPB * NQ;                                // [CPB][NN]
+    double *sJz = sJac + CPB * NN;                               // [CPB][NN]  Jz^2 for the sensor
     double *sLow = sJz + CPB * NN;                               // [CPB][kLow]
     double *sRed = sLow + CPB * S::kLow;                         // [4][32] block reductions
     double *sRes = sRed + 4 * 32;                                // [CPB][NQ] residual
-    R *sF = reinterpret_cast<R *>(sRes + CPB * NQ);              // [CPB][2][N][NP][9]
+    R *sNrm = reinterpret_cast<R *>(sRes + CPB * NQ);            // [CPB][NM] flux-point normals
+    R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
     R *sV = sF + CPB * S::kF;                                    // [CPB][2][N][NP][NG]
-    R *sQr = sV + CPB * S::kV;                                   // [CPB][NQ] (float form only)
 
     const int tid = threadIdx.x;
     const int c0 = blockIdx.x * CPB;
@@ -201,25 +202,25 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         for (int k = tid; k < n; k += NT) sQ[k] = __ldg(src + k);
         const double *msrc = a.met + (size_t)c0 * ML::kSize;
         const int nm = ncl * ML::kSize;
-        for (int k = tid; k < nm; k += NT) sMet[k] = __ldg(msrc + k);
+        for (int k = tid; k < nm; k += NT) {
+            const int c = k / ML::kSize, o = k - c * ML::kSize;
+            const double v = __ldg(msrc + k);
+            if (o < NM) sNrm[c * NM + o] = (R)v;  // rounded once to the arithmetic type
+            else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
+        }
     }
     const double eig_r = a.maxima[2 * a.slot_r], um_r = a.maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
     const R c_h = (R)sqrt(eig_r * (eig_r - um_r));
     __syncthreads();
-    if constexpr (sizeof(R) != sizeof(double)) {
-        for (int k = tid; k < ncl * NQ; k += NT) sQr[k] = (R)sQ[k];
-        __syncthreads();
-    }
-    const R *qsrc = (sizeof(R) == sizeof(double)) ? reinterpret_cast<const R *>(sQ) : sQr;
 
     // ---- A: interpolate every line to its flux points ---------------------------
     for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
         const int v = t % 9, l = (t / 9) % N, f = (t / (9 * N)) % 2, c = t / (18 * N);
-        const R *q = qsrc + c * NQ;
+        const double *q = sQ + c * NQ;
         R qs[N];
 #pragma unroll
-        for (int s = 0; s < N; s++) qs[s] = f == 0 ? q[v + 9 * (s + N * l)] : q[v + 9 * (l + N * s)];
+        for (int s = 0; s < N; s++) qs[s] = (R)(f == 0 ? q[v + 9 * (s + N * l)] : q[v + 9 * (l + N * s)]);
         R *out = sF + c * S::kF + (f * N + l) * NP * 9 + v;
 #pragma unroll
         for (int r = 0; r < NP; r++) {
@@ -244,8 +245,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         for (int k = 0; k < 9; k++) q[k] = slot[k];
         if (!(q[0] > (R)0)) err |= kErrNonPositiveDensity;
         iflux<R, EX>(q, c_h, umax, F, G);
-        const double *nrm = sMet + c * ML::kSize + ML::normal(f, l, r);
-        const R n0 = (R)nrm[0], n1 = (R)nrm[1];
+        const R *nrm = sNrm + c * NM + ML::normal(f, l, r);
+        const R n0 = nrm[0], n1 = nrm[1];
 #pragma unroll
         for (int k = 0; k < 9; k++) slot[k] = F[k] * n0 + G[k] * n1;
         R *vs = sV + c * S::kV + ((f * N + l) * NP + r) * NG;
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         for (int k = 0; k < 9; k++) own[k] = slot[k];
         const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
         const int kind = rec.y & 0xff;
-        const double *onrm = sMet + c * ML::kSize + ML::normal(fam, line, r);
+        const R *onrm = sNrm + c * NM + ML::normal(fam, line, r);
         R n0, n1;
         int sign_l, sign_r;
         const bool pair = kind == kFaceLeft || kind == kFaceRight;
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int k = 0; k < 9; k++) other[k] = tp[k];
             if (!own_right) {
-                n0 = (R)onrm[0]; n1 = (R)onrm[1];
+                n0 = onrm[0]; n1 = onrm[1];
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = pr == N ? -1 : 1;
             } else {
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 sign_r = r == N ? -1 : 1;
             }
         } else {
-            n0 = (R)onrm[0]; n1 = (R)onrm[1];
+            n0 = onrm[0]; n1 = onrm[1];
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
             bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.fs, other);
@@ -331,8 +332,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
         const int cell = c0 + c;
-        const double *met = sMet + c * ML::kSize;
-        const double J = met[ML::kJac + i + N * j];
+        const R *met = sNrm + c * NM;
+        const double J = sJac[c * NN + i + N * j];
         const R *Fx = sF + c * S::kF + (0 * N + j) * NP * 9;  // xi-line j
         const R *Fy = sF + c * S::kF + (1 * N + i) * NP * 9;  // eta-line i
         const R *Vx = sV + c * S::kV + (0 * N + j) * NP * NG;
@@ -354,14 +355,14 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int r = 0; r < NP; r++) {
                 const R mx = Vx[r * NG + g] * opM<R>(ops, r * N + i);
-                ax = ax + mx * (R)met[ML::normal(0, j, r)];
-                ay = ay + mx * (R)met[ML::normal(0, j, r) + 1];
+                ax = ax + mx * met[ML::normal(0, j, r)];
+                ay = ay + mx * met[ML::normal(0, j, r) + 1];
             }
 #pragma unroll
             for (int r = 0; r < NP; r++) {
                 const R my = Vy[r * NG + g] * opM<R>(ops, r * N + j);
-                bx = bx + my * (R)met[ML::normal(1, i, r)];
-                by = by + my * (R)met[ML::normal(1, i, r) + 1];
+                bx = bx + my * met[ML::normal(1, i, r)];
+                by = by + my * met[ML::normal(1, i, r) + 1];
             }
             double gx, gy;
             if constexpr (EX) {
@@ -442,33 +443,72 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     const bool av = a.artiv == 1 && a.vismode == 1;
     if (av) {
         constexpr int NL = N - 1;
-        for (int t = tid; t < ncl * 2 * NL * NL; t += NT) {
-            const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
-            const double *q = sQ + c * NQ;
-            const double *jz = sJz + c * NN;
-            double acc = 0.0;
-            for (int js = 0; js < N; js++)
+        // the sensed fields: density (v = 0) and Jz^2 (v = 1)
+        auto field = [&](int c, int v, int is, int js) -> double {
+            return v == 0 ? sQ[c * NQ + 9 * (is + N * js)] : sJz[c * NN + is + N * js];
+        };
+        // the flux buffer is free after phase C: it holds the separable
+        // projection's intermediate products
+        double *sTmp = reinterpret_cast<double *>(sF);  // [CPB][2][NL][N]
+        if constexpr (EX) {
+            // projection to the N-1 points with the reference's double sum
+            for (int t = tid; t < ncl * 2 * NL * NL; t += NT) {
+                const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
+                double acc = 0.0;
+                for (int js = 0; js < N; js++)
 #pragma unroll
-                for (int is = 0; is < N; is++) {
-                    const double x = v == 0 ? q[9 * (is + N * js)] : jz[is + N * js];
-                    acc = acc + x * ops.H[isl * N + is] * ops.H[jsl * N + js];
-                }
-            sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
+                    for (int is = 0; is < N; is++)
+                        acc = acc + field(c, v, is, js) * ops.H[isl * N + is] * ops.H[jsl * N + js];
+                sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
+            }
+        } else {
+            // the same projection as two one-dimensional passes
+            for (int t = tid; t < ncl * 2 * NL * N; t += NT) {
+                const int isl = t % NL, js = (t / NL) % N, v = (t / (NL * N)) % 2, c = t / (2 * NL * N);
+                double acc = 0.0;
+#pragma unroll
+                for (int is = 0; is < N; is++) acc += field(c, v, is, js) * ops.H[isl * N + is];
+                sTmp[((c * 2 + v) * N + js) * NL + isl] = acc;
+            }
+            __syncthreads();
+            for (int t = tid; t < ncl * 2 * NL * NL; t += NT) {
+                const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
+                double acc = 0.0;
+#pragma unroll
+                for (int js = 0; js < N; js++) acc += sTmp[((c * 2 + v) * N + js) * NL + isl] * ops.H[jsl * N + js];
+                sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
+            }
         }
         __syncthreads();
         // projection back to the solution points and the terms of the sensor
         // sum, one thread per (cell, variable, point); the face-state buffer
         // is free after phase C and holds the terms
         double *sTerm = reinterpret_cast<double *>(sV);  // [CPB][2][NN]
+        if constexpr (!EX) {
+            for (int t = tid; t < ncl * 2 * N * NL; t += NT) {
+                const int is = t % N, jsl = (t / N) % NL, v = (t / (N * NL)) % 2, c = t / (2 * N * NL);
+                const double *lo = sLow + c * S::kLow + v * NL * NL;
+                double acc = 0.0;
+#pragma unroll
+                for (int isl = 0; isl < NL; isl++) acc += lo[isl + NL * jsl] * ops.HL[is * NL + isl];
+                sTmp[((c * 2 + v) * NL + jsl) * N + is] = acc;
+            }
+            __syncthreads();
+        }
         for (int t = tid; t < ncl * 2 * NN; t += NT) {
             const int is = t % N, js = (t / N) % N, v = (t / NN) % 2, c = t / (2 * NN);
-            const double *lo = sLow + c * S::kLow + v * NL * NL;
             double hi = 0.0;
-            for (int jsl = 0; jsl < NL; jsl++)
+            if constexpr (EX) {
+                const double *lo = sLow + c * S::kLow + v * NL * NL;
+                for (int jsl = 0; jsl < NL; jsl++)
 #pragma unroll
-                for (int isl = 0; isl < NL; isl++)
-                    hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
-            const double x = v == 0 ? sQ[c * NQ + 9 * (is + N * js)] : sJz[c * NN + is + N * js];
+                    for (int isl = 0; isl < NL; isl++)
+                        hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
+            } else {
+#pragma unroll
+                for (int jsl = 0; jsl < NL; jsl++) hi += sTmp[((c * 2 + v) * NL + jsl) * N + is] * ops.HL[js * NL + jsl];
+            }
+            const double x = field(c, v, is, js);
             const double d = hi - x;
             sTerm[(c * 2 + v) * NN + is + N * js] = d * d / (x * x);
         }
@@ -515,18 +555,20 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     if (!DIAG && a.t_out) {
         __syncthreads();
         R *to = reinterpret_cast<R *>(a.t_out) + (size_t)c0 * 4 * N * 9;
-        for (int t = tid; t < ncl * 4 * N * 9; t += NT) {
-            const int k = t % 9, nfp = 1 + (t / 9) % N, lf = 1 + (t / (9 * N)) % 4, c = t / (36 * N);
+        for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
+            const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
             int fam, line, r;
             face_point<N>(lf, nfp, fam, line, r);
-            const double *q = sQ + c * NQ;
-            R acc = (R)0;
+            const double *q = sQ + c * NQ + (fam == 0 ? 9 * N * line : 9 * line);
+            const int stride = fam == 0 ? 9 : 9 * N;
+            R *o = to + (size_t)t * 9;
 #pragma unroll
-            for (int s = 0; s < N; s++) {
-                const double x = fam == 0 ? q[k + 9 * (s + N * line)] : q[k + 9 * (line + N * s)];
-                acc = acc + (R)x * opL<R>(ops, r * N + s);
+            for (int k = 0; k < 9; k++) {
+                R acc = (R)0;
+#pragma unroll
+                for (int s = 0; s < N; s++) acc = acc + (R)q[k + stride * s] * opL<R>(ops, r * N + s);
+                o[k] = acc;
             }
-            to[t] = acc;
         }
     }
 
