@@ -130,6 +130,52 @@ int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev);
    callers that order their own work or CUDA events against the drop-in. */
 int sddc_get_stream(sddc_ctx *ctx, void **stream);
 
+/* ---- residual evaluation without device allocation ----------------------
+   No counterpart in the reference.  For callers that cannot call cudaMalloc:
+   a host that hands out all device memory from its own pool or budget, code
+   running while a stream is being captured into a CUDA graph, a plugin
+   inside a framework that owns the allocator.  The caller passes all inputs
+   and outputs as device memory it holds; the working memory (face traces,
+   running-maxima slots, AV sensor, fault flags) is one fixed array of
+   SDDC_NOALLOC_SCRATCH_BYTES bytes inside the library, which every GPU that
+   loads the library keeps until the process exits.  A case whose working
+   memory exceeds it (about 11,000 cells at N = 5 in FP64, 14,000 at N = 4)
+   is rejected with SDDC_EINVAL.  All calls share the array: calls that
+   overlap on the GPU (several host threads, several streams) race; the
+   array keeps the last call's contents and each call rewrites what it
+   reads.  The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress); make it before any stream capture on that device. */
+#define SDDC_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+
+size_t sddc_noalloc_scratch_bytes(void);
+const char *sddc_noalloc_last_error(void);
+
+/* Sizes of the packed tables: met_doubles doubles of metrics and
+   face_ints ints of (cell, local face) records. */
+int sddc_noalloc_packed_sizes(int N, int ncell, size_t *met_doubles, size_t *face_ints);
+
+/* Packs the reference-layout tables (as for sddc_set_tables) into caller
+   host buffers of the sizes above; the caller copies them to the device. */
+int sddc_noalloc_pack_tables(int N, int ncell, const double *S1, const double *S2, const double *Jac,
+                             const int *IF2C, int nface, const int *ibfinter, int ninter,
+                             const int *ibfinl, int ninlet, const int *ibfout, int noutlet,
+                             const int *ibfwal, int nwall, const int *ibfsymp, int nsymp,
+                             const int *ibfree, int nfree, const int *cyc2fpair, int npair,
+                             double *met_out, int *faces_out);
+
+/* One residual evaluation of q_dev (9,N,N,NCELL) on `stream` (NULL: the
+   default stream), as sddc_compresid: writes resid_dev (9,N,N,NCELL) and
+   nablaqs_dev (9,2,N,N,NCELL), both device memory of the caller.  eigvmax
+   and umax are the running maxima before the evaluation (0 at start);
+   maxima_out[0..1] receives them after it (pass them to the next call).
+   Lmat and Mmat are host arrays (N+1,N).  Synchronises the stream before it
+   returns; allocates no device memory.  p->cells_per_cta and p->k_stage
+   are ignored. */
+int sddc_compresid_noalloc(const sddc_params *p, const double *Lmat, const double *Mmat,
+                           const double *q_dev, const double *met_dev, const int *faces_dev,
+                           double eigvmax, double umax, double *resid_dev, double *nablaqs_dev,
+                           double *maxima_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,7 @@ CUDA_UNITS = {
     "stage_fp64.cu": [],
     "stage_mixed.cu": [],
     "context.cu": [],
+    "noalloc.cu": [],
 }
 
 
