@@ -243,8 +243,10 @@ def run_ours(args):
         "mixed_vs_fp64_exact_rel_l2": float(np.linalg.norm(states["mixed"] - ref) / np.linalg.norm(ref)),
         "fp64_vs_fp64_exact_rel_l2": float(np.linalg.norm(states["fp64"] - ref) / np.linalg.norm(ref)),
         "after_steps": steps + warm,
-        "note": "fp64_exact is bit-equal to the CPU oracle (tests/test_gpu_parity.py)",
+        "note": "fp64_exact is bit-equal to the CPU oracle (tests/test_gpu_parity.py, test_gpu_fullsize.py)",
     }
+    if args.accuracy_steps:
+        acc["long_run"] = accuracy_run(solver_mod, t, ph, Q0, dt, dof, args.accuracy_steps)
     units = dof * 5 * steps
     val = {k: world * units / (v / 1e3) for k, v in results.items()}
     peak, peak_kind = measured_peaks()
@@ -296,6 +298,36 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def accuracy_run(solver_mod, t, ph, Q0, dt, dof, nsteps):
+    """The mixed and FP64 forms against the FP64-exact form (bit-equal to
+    the CPU oracle) after `nsteps` RK3 steps: rel-L2 of each variable, the
+    divB L2 norm and the change of the integrated density."""
+    out = {}
+    for prec in ("fp64_exact", "fp64", "mixed"):
+        s = solver_mod.Solver(t, ph, precision=prec, cells_per_cta=TILES.get(prec, {}).get("cells_per_cta", 0))
+        s.set_state(Q0)
+        m0 = s.monitor()["mass"]
+        s.rk_s5p3(dt, nsteps)
+        mon = s.monitor()
+        out[prec] = (s.state()["Q"], m0, mon)
+        s.close()
+    ref, m0, mref = out["fp64_exact"]
+    res = {"steps": nsteps, "t_end": nsteps * dt, "finite": bool(np.isfinite(ref).all()),
+           "divB_l2_fp64_exact": float(np.sqrt(mref["divbsum"] / dof)),
+           "mass_change_fp64_exact": (mref["mass"] - m0) / m0}
+    names = ["rho", "rhou", "rhov", "rhow", "E", "Bx", "By", "Bz", "psi"]
+    for prec in ("fp64", "mixed"):
+        q, m0p, mon = out[prec]
+        res[prec] = {
+            "rel_l2_all": float(np.linalg.norm(q - ref) / np.linalg.norm(ref)),
+            "rel_l2_per_var": {n: float(np.linalg.norm(q[k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))
+                               for k, n in enumerate(names)},
+            "divB_l2": float(np.sqrt(mon["divbsum"] / dof)),
+            "mass_change_minus_exact": (mon["mass"] - m0p) / m0p - res["mass_change_fp64_exact"],
+        }
+    return res
 
 
 def cpu_baseline(t, ph, Q0, dt, dof, steps=1):
@@ -358,6 +390,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["mixed", "fp64", "fp64_exact"], default=None,
                     help="time one form only (the command used for ncu captures)")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="RK3 steps of the mixed/FP64 vs FP64-exact comparison (0: skip)")
     ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8, 16],
                     help="cells per CTA; 0 lets the autotuner choose")
     args = ap.parse_args()
