@@ -150,8 +150,8 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    size_t d = (size_t)CPB * (2 * S::NQ + 2 * N * N + S::kLow) + 4 * 32;
-    size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam);
+    size_t d = (size_t)CPB * (2 * S::NQ + 2 * N * N + S::kLow) + 4 * 32 + 2 * (N - 1) * N;
+    size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam) + 2 * (N + 1) * N;
     return d * sizeof(double) + r * sizeof(R);
 }
 
@@ -187,15 +187,29 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *sLow = sJz + CPB * NN;                               // [CPB][kLow]
     double *sRed = sLow + CPB * S::kLow;                         // [4][32] block reductions
     double *sRes = sRed + 4 * 32;                                // [CPB][NQ] residual
-    R *sNrm = reinterpret_cast<R *>(sRes + CPB * NQ);            // [CPB][NM] flux-point normals
+    double *sOpH = sRes + CPB * NQ;                              // [N-1][N]  AV projection
+    double *sOpHL = sOpH + (N - 1) * N;                          // [N][N-1]  AV prolongation
+    R *sNrm = reinterpret_cast<R *>(sOpHL + N * (N - 1));        // [CPB][NM] flux-point normals
     R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
     R *sV = sF + CPB * S::kF;                                    // [CPB][2][N][NP][NG]
+    // operators read with lane-dependent indices live in shared memory
+    // (divergent reads of kernel parameters serialise per address)
+    R *sOpL = sV + CPB * S::kV;                                  // [NP][N]
+    R *sOpM = sOpL + NP * N;                                     // [NP][N]
 
     const int tid = threadIdx.x;
     const int c0 = blockIdx.x * CPB;
     const int ncl = min(CPB, a.ncell - c0);  // cells of this CTA
 
-    // ---- stage the state and the metrics ------------------------------------
+    // ---- stage the state, the metrics and the operators ------------------------
+    for (int k = tid; k < NP * N; k += NT) {
+        sOpL[k] = opL<R>(ops, k);
+        sOpM[k] = opM<R>(ops, k);
+    }
+    for (int k = tid; k < (N - 1) * N; k += NT) {
+        sOpH[k] = ops.H[k];
+        sOpHL[k] = ops.HL[k];
+    }
     {
         const double *src = a.q_in + (size_t)c0 * NQ;
         const int n = ncl * NQ;
@@ -354,13 +368,13 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             R ax = (R)0, ay = (R)0, bx = (R)0, by = (R)0;
 #pragma unroll
             for (int r = 0; r < NP; r++) {
-                const R mx = Vx[r * NG + g] * opM<R>(ops, r * N + i);
+                const R mx = Vx[r * NG + g] * sOpM[r * N + i];
                 ax = ax + mx * met[ML::normal(0, j, r)];
                 ay = ay + mx * met[ML::normal(0, j, r) + 1];
             }
 #pragma unroll
             for (int r = 0; r < NP; r++) {
-                const R my = Vy[r * NG + g] * opM<R>(ops, r * N + j);
+                const R my = Vy[r * NG + g] * sOpM[r * N + j];
                 bx = bx + my * met[ML::normal(1, i, r)];
                 by = by + my * met[ML::normal(1, i, r) + 1];
             }
@@ -394,8 +408,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             R dF = (R)0, dG = (R)0;
 #pragma unroll
             for (int r = 0; r < NP; r++) {
-                dF = dF + Fx[r * 9 + k] * opM<R>(ops, r * N + i);
-                dG = dG + Fy[r * 9 + k] * opM<R>(ops, r * N + j);
+                dF = dF + Fx[r * 9 + k] * sOpM[r * N + i];
+                dG = dG + Fy[r * 9 + k] * sOpM[r * N + j];
             }
             res[k] = (double)(-(dF + dG));
             // the viscous chain adds exactly +0.0 when mu == eta0 == 0
@@ -458,7 +472,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 for (int js = 0; js < N; js++)
 #pragma unroll
                     for (int is = 0; is < N; is++)
-                        acc = acc + field(c, v, is, js) * ops.H[isl * N + is] * ops.H[jsl * N + js];
+                        acc = acc + field(c, v, is, js) * sOpH[isl * N + is] * sOpH[jsl * N + js];
                 sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
             }
         } else {
@@ -467,7 +481,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 const int isl = t % NL, js = (t / NL) % N, v = (t / (NL * N)) % 2, c = t / (2 * NL * N);
                 double acc = 0.0;
 #pragma unroll
-                for (int is = 0; is < N; is++) acc += field(c, v, is, js) * ops.H[isl * N + is];
+                for (int is = 0; is < N; is++) acc += field(c, v, is, js) * sOpH[isl * N + is];
                 sTmp[((c * 2 + v) * N + js) * NL + isl] = acc;
             }
             __syncthreads();
@@ -475,7 +489,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 const int isl = t % NL, jsl = (t / NL) % NL, v = (t / (NL * NL)) % 2, c = t / (2 * NL * NL);
                 double acc = 0.0;
 #pragma unroll
-                for (int js = 0; js < N; js++) acc += sTmp[((c * 2 + v) * N + js) * NL + isl] * ops.H[jsl * N + js];
+                for (int js = 0; js < N; js++) acc += sTmp[((c * 2 + v) * N + js) * NL + isl] * sOpH[jsl * N + js];
                 sLow[c * S::kLow + v * NL * NL + isl + NL * jsl] = acc;
             }
         }
@@ -490,7 +504,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 const double *lo = sLow + c * S::kLow + v * NL * NL;
                 double acc = 0.0;
 #pragma unroll
-                for (int isl = 0; isl < NL; isl++) acc += lo[isl + NL * jsl] * ops.HL[is * NL + isl];
+                for (int isl = 0; isl < NL; isl++) acc += lo[isl + NL * jsl] * sOpHL[is * NL + isl];
                 sTmp[((c * 2 + v) * NL + jsl) * N + is] = acc;
             }
             __syncthreads();
@@ -503,10 +517,10 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 for (int jsl = 0; jsl < NL; jsl++)
 #pragma unroll
                     for (int isl = 0; isl < NL; isl++)
-                        hi = hi + lo[isl + NL * jsl] * ops.HL[is * NL + isl] * ops.HL[js * NL + jsl];
+                        hi = hi + lo[isl + NL * jsl] * sOpHL[is * NL + isl] * sOpHL[js * NL + jsl];
             } else {
 #pragma unroll
-                for (int jsl = 0; jsl < NL; jsl++) hi += sTmp[((c * 2 + v) * NL + jsl) * N + is] * ops.HL[js * NL + jsl];
+                for (int jsl = 0; jsl < NL; jsl++) hi += sTmp[((c * 2 + v) * NL + jsl) * N + is] * sOpHL[js * NL + jsl];
             }
             const double x = field(c, v, is, js);
             const double d = hi - x;
@@ -566,7 +580,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             for (int k = 0; k < 9; k++) {
                 R acc = (R)0;
 #pragma unroll
-                for (int s = 0; s < N; s++) acc = acc + (R)q[k + stride * s] * opL<R>(ops, r * N + s);
+                for (int s = 0; s < N; s++) acc = acc + (R)q[k + stride * s] * sOpL[r * N + s];
                 o[k] = acc;
             }
         }
