@@ -341,7 +341,27 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     }
     __syncthreads();
 
-    // ---- C: divergence, B gradient, sources, RK update --------------------------
+    // ---- C1: flux derivative along every line, in place ------------------------
+    // one thread per (cell, family, line, variable): the N+1 flux values of
+    // the line, d(i) = sum over r of F(r) * M(r, i) in the reference's order
+    // (compresid.f90:14-32), written over point slots 0..N-1 of the line
+    for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
+        const int k = t % 9, l = (t / 9) % N, f = (t / (9 * N)) % 2, c = t / (18 * N);
+        R *col = sF + c * S::kF + (f * N + l) * NP * 9 + k;
+        R fv[NP];
+#pragma unroll
+        for (int r = 0; r < NP; r++) fv[r] = col[r * 9];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            R d = (R)0;
+#pragma unroll
+            for (int r = 0; r < NP; r++) d = d + fv[r] * opM<R>(ops, r * N + i);
+            col[i * 9] = d;
+        }
+    }
+    __syncthreads();
+
+    // ---- C: B gradient, sources and the residual per solution point ------------
     double part_r = 0.0, part_d = 0.0;
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
@@ -401,16 +421,12 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             const double d = gB[1][0] - gB[0][1];
             sJz[c * NN + i + N * j] = d * d;
         }
-        // compresid.f90:12-51 divergence of the inviscid flux
+        // compresid.f90:12-51 divergence of the inviscid flux: the line sums
+        // of phase C1 sit in point slot i of xi-line j and slot j of eta-line i
         double res[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) {
-            R dF = (R)0, dG = (R)0;
-#pragma unroll
-            for (int r = 0; r < NP; r++) {
-                dF = dF + Fx[r * 9 + k] * sOpM[r * N + i];
-                dG = dG + Fy[r * 9 + k] * sOpM[r * N + j];
-            }
+            const R dF = Fx[i * 9 + k], dG = Fy[j * 9 + k];
             res[k] = (double)(-(dF + dG));
             // the viscous chain adds exactly +0.0 when mu == eta0 == 0
             if (a.vismode == 1) res[k] = res[k] + 0.0;
@@ -561,6 +577,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 a.q_out[g] = o;
                 if (a.resid_w) a.resid_w[g] = r;
                 sQ[e] = o;  // the sensor read sQ before the barrier above
+                // the float form keeps the output in its arithmetic type for
+                // phase F (the flux buffer is free by now)
+                if constexpr (sizeof(R) != sizeof(double)) reinterpret_cast<R *>(sF)[e] = (R)o;
             }
         }
     }
@@ -573,7 +592,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
             int fam, line, r;
             face_point<N>(lf, nfp, fam, line, r);
-            const double *q = sQ + c * NQ + (fam == 0 ? 9 * N * line : 9 * line);
+            const R *q = (sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(sQ) : reinterpret_cast<const R *>(sF)) +
+                         c * NQ + (fam == 0 ? 9 * N * line : 9 * line);
             const int stride = fam == 0 ? 9 : 9 * N;
             R *o = to + (size_t)t * 9;
 #pragma unroll
