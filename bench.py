@@ -293,6 +293,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(Q0.nbytes), "d2h_bytes_per_step": int(Q0.nbytes) + 32,
                 "steps": e2e_steps, "path": "sddc_set_state + sddc_rk_step + sddc_get_state + sddc_monitor"},
         "gpu_launches": 5 * steps,
+        "ensemble": ensemble_run(torch) if not args.no_ensemble else None,
     }
     print(json.dumps(line))
     if dist:
@@ -328,6 +329,63 @@ def accuracy_run(solver_mod, t, ph, Q0, dt, dof, nsteps):
             "mass_change_minus_exact": (mon["mass"] - m0p) / m0p - res["mass_change_fp64_exact"],
         }
     return res
+
+
+def ensemble_run(torch, ncase=64, steps=20, warmup=3, seed=0):
+    """64 cylinder cases (p = 3, mixed, sizes uniform over 16x32..128x256,
+    per-case CFL time steps) in one launch per stage, against the same cases
+    run one after another, each on its own context."""
+    from sddc_b200 import autotune, ensemble
+
+    members = ensemble.build_members(ensemble.make_cases(ncase, seed=seed))
+    dof_total = sum(m.tables.ncell * m.tables.N ** 2 for m in members)
+
+    def timed(run, stream_handle):
+        st = torch.cuda.ExternalStream(stream_handle)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        run()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    # tile for the batch (untimed tuning on the batch itself)
+    best, best_t = 4, None
+    for cpb in (4, 8, 16):
+        b = ensemble.Batch(members, precision="mixed", cells_per_cta=cpb)
+        b.reset()
+        b.step(2)
+        tt = timed(lambda: b.step(3), b.solver.stream_handle())
+        if best_t is None or tt < best_t:
+            best, best_t = cpb, tt
+        b.close()
+    b = ensemble.Batch(members, precision="mixed", cells_per_cta=best)
+    b.reset()
+    b.step(warmup)
+    t_batch = timed(lambda: b.step(steps), b.solver.stream_handle())
+    qb = b.solver.state()["Q"]
+    finite = bool(np.isfinite(qb).all())
+    b.close()
+    t_seq = 0.0
+    from sddc_b200.solver import Solver
+
+    for m in members:
+        cpb, _ = autotune.tune(m.tables, m.case.physics, m.Q0, m.dt, "mixed", steps=2)
+        s = Solver(m.tables, m.case.physics, precision="mixed", cells_per_cta=cpb)
+        s.set_state(m.Q0)
+        s.rk_s5p3(m.dt, warmup)
+        t_seq += timed(lambda: s.rk_s5p3(m.dt, steps), s.stream_handle())
+        s.close()
+    units = dof_total * 5 * steps
+    sizes = {}
+    for m in members:
+        key = f"{m.case.mesh.ncell}"
+        sizes[key] = sizes.get(key, 0) + 1
+    return {"cases": ncase, "dof_total": dof_total, "cells_by_case_size": sizes, "steps": steps,
+            "form": "mixed", "cells_per_cta": best, "finite": finite,
+            "batched": {"value": units / t_batch, "unit": UNIT, "s_per_step": t_batch / steps},
+            "sequential": {"value": units / t_seq, "unit": UNIT, "s_per_step": t_seq / steps},
+            "batched_over_sequential": t_seq / t_batch}
 
 
 def cpu_baseline(t, ph, Q0, dt, dof, steps=1):
@@ -388,6 +446,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-case batched ensemble block")
     ap.add_argument("--only", choices=["mixed", "fp64", "fp64_exact"], default=None,
                     help="time one form only (the command used for ncu captures)")
     ap.add_argument("--accuracy-steps", type=int, default=2000,

@@ -130,6 +130,28 @@ int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev);
    callers that order their own work or CUDA events against the drop-in. */
 int sddc_get_stream(sddc_ctx *ctx, void **stream);
 
+/* ---- batches of independent cases ----------------------------------------
+   No counterpart in the reference (its runs are one case each).  Several
+   cases of the same N and form share one context: their tables are
+   concatenated (cells, faces and face lists renumbered so that case k owns
+   cells first_cell .. first_cell+ncell-1), and every stage is one launch
+   over all of them, tiled so that no CTA straddles two cases.  Each case
+   keeps its own free stream, time step and running maxima (c_h). */
+typedef struct sddc_case {
+    int first_cell;  /* 0-based first cell of the case in the concatenation */
+    int ncell;
+    double dt;
+    double rinf, pinf, uinf, vinf, bxinf, byinf;
+} sddc_case;
+
+/* After sddc_set_tables on the concatenated tables; resets the running
+   maxima, so sddc_set_state follows. */
+int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases);
+/* nsteps time steps of every case with its own dt. */
+int sddc_rk_step_cases(sddc_ctx *ctx, int nsteps);
+/* Running maxima of one case after the last evaluation. */
+int sddc_get_case_maxima(sddc_ctx *ctx, int icase, double *eigvmax, double *umax);
+
 /* ---- residual evaluation without device allocation ----------------------
    No counterpart in the reference.  For callers that cannot call cudaMalloc:
    a host that hands out all device memory from its own pool or budget, code

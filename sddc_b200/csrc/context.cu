@@ -192,6 +192,12 @@ struct sddc_ctx {
     double ctime = 0.0;
     cudaGraphExec_t graph[kSlots] = {};
     double graph_dt[kSlots] = {};
+    // batch of independent cases (sddc_set_cases); ncase == 0 for one case
+    int ncase = 0;
+    std::vector<sddc_case> cases;
+    CaseParams *case_dev = nullptr;
+    int4 *tiles_rk = nullptr, *tiles_diag = nullptr;
+    int ntiles_rk = 0, ntiles_diag = 0;
 };
 
 static int set_err(sddc_ctx *c, int code, const std::string &m)
@@ -223,7 +229,8 @@ static void free_all(sddc_ctx *ctx)
     for (auto &r : ctx->reg) cudaFree(r), r = nullptr;
     for (auto &t : ctx->trace) cudaFree(t), t = nullptr;
     void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
-                    ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags};
+                    ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags,
+                    ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag};
     for (void *b : bufs) cudaFree(b);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -430,12 +437,13 @@ extern "C" int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, doub
 {
     if (!ctx || !Q) return set_err(ctx, SDDC_EINVAL, "sddc_set_state: NULL argument");
     CK(cudaMemcpyAsync(ctx->reg[0], Q, ctx->nq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    double mx[2 * kSlots];
-    for (int s = 0; s < kSlots; s++) {
+    // every running-max slot of every case starts from the given maxima
+    std::vector<double> mx(2 * kSlots * std::max(ctx->ncase, 1));
+    for (size_t s = 0; s < mx.size() / 2; s++) {
         mx[2 * s] = eigvmax;
         mx[2 * s + 1] = umax;
     }
-    CK(cudaMemcpyAsync(ctx->maxima, mx, sizeof(mx), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->maxima, mx.data(), mx.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if (ctx->tables) {
         int rc = refresh_traces(ctx);
         if (rc) return rc;
@@ -465,8 +473,14 @@ static StageArgs base_args(sddc_ctx *ctx)
     return a;
 }
 
-static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a)
+static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a_in)
 {
+    StageArgs a = a_in;
+    if (ctx->ncase) {  // a batch: one CTA per tile of the case-aligned tile table
+        a.tiles = diag ? ctx->tiles_diag : ctx->tiles_rk;
+        a.ntiles = diag ? ctx->ntiles_diag : ctx->ntiles_rk;
+        a.cases = ctx->case_dev;
+    }
     switch (ctx->p.precision) {
     case SDDC_FP64_EXACT: return launch_stage_exact(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
     case SDDC_FP64: return launch_stage_fp64(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
@@ -522,7 +536,7 @@ extern "C" int sddc_compresid(sddc_ctx *ctx)
     a.mon_part = ctx->mon_part;
     CK(launch(ctx, true, a));
     ctx->slot = a.slot_w;
-    ctx->mon_nblk = (ctx->ncell + 7) / 8;
+    ctx->mon_nblk = ctx->ncase ? ctx->ntiles_diag : (ctx->ncell + 7) / 8;
     CK(cudaStreamSynchronize(ctx->stream));
     return check_flags(ctx);
 }
@@ -532,24 +546,28 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
 {
     double **P = ctx->reg;
     StageArgs a = base_args(ctx);
+    a.dt = dt;
+    // stage table: kind, registers, base coefficients and which of them are
+    // multiplied by the case's dt (in the kernel, as the host would)
     struct St {
         int kind;
         int in, out, ra, rb, rc, rd, rw;
         double c[6];
+        unsigned mask;
     };
     St st[5];
     if (ctx->p.k_stage == 3) {  // RK_S5P3, iterations.f90:179-210
-        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {B10 * dt}};
-        st[1] = {kRkAxpy, 1, 2, -1, -1, -1, -1, -1, {B21 * dt}};
-        st[2] = {kRkTwoReg, 2, 1, 0, -1, -1, -1, -1, {B32 * dt, A30, A32}};
-        st[3] = {kRkTwoReg, 1, 3, 0, -1, -1, -1, -1, {B43 * dt, A40, A43}};
-        st[4] = {kRkTwoReg, 3, 0, 2, -1, -1, -1, -1, {B54 * dt, A52, A54}};
+        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {B10}, 1u};
+        st[1] = {kRkAxpy, 1, 2, -1, -1, -1, -1, -1, {B21}, 1u};
+        st[2] = {kRkTwoReg, 2, 1, 0, -1, -1, -1, -1, {B32, A30, A32}, 1u};
+        st[3] = {kRkTwoReg, 1, 3, 0, -1, -1, -1, -1, {B43, A40, A43}, 1u};
+        st[4] = {kRkTwoReg, 3, 0, 2, -1, -1, -1, -1, {B54, A52, A54}, 1u};
     } else {  // FiveStageRk, iterations.f90:103-152
-        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {dt * F11}};
-        st[1] = {kRkTwoRegT, 1, 2, 0, -1, -1, -1, -1, {F23, F21, F22, dt}};
-        st[2] = {kRkTwoReg, 2, 3, 0, -1, -1, -1, -1, {F33 * dt, F31, F32}};
-        st[3] = {kRkTwoReg, 3, 4, 0, -1, -1, -1, 5, {F43 * dt, F41, F42}};
-        st[4] = {kRkFive, 4, 0, 0, 2, 3, 5, -1, {F56 * dt, F51, F52, F53, F54, F55 * dt}};
+        st[0] = {kRkAxpy, 0, 1, -1, -1, -1, -1, -1, {F11}, 1u};
+        st[1] = {kRkTwoRegT, 1, 2, 0, -1, -1, -1, -1, {F23, F21, F22, 1.0}, 8u};
+        st[2] = {kRkTwoReg, 2, 3, 0, -1, -1, -1, -1, {F33, F31, F32}, 1u};
+        st[3] = {kRkTwoReg, 3, 4, 0, -1, -1, -1, 5, {F43, F41, F42}, 1u};
+        st[4] = {kRkFive, 4, 0, 0, 2, 3, 5, -1, {F56, F51, F52, F53, F54, F55}, 1u | 32u};
     }
     for (int k = 0; k < 5; k++) {
         a.rk_kind = st[k].kind;
@@ -562,7 +580,8 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
         a.reg_c = st[k].rc >= 0 ? P[st[k].rc] : nullptr;
         a.reg_d = st[k].rd >= 0 ? P[st[k].rd] : nullptr;
         a.resid_w = st[k].rw >= 0 ? P[st[k].rw] : nullptr;
-        for (int i = 0; i < 6; i++) a.c[i] = st[k].c[i];
+        for (int i = 0; i < 6; i++) a.cb[i] = st[k].c[i];
+        a.dt_mask = st[k].mask;
         a.slot_r = (s0 + k) % kSlots;
         a.slot_w = (s0 + k + 1) % kSlots;
         a.mon_part = k == 4 ? ctx->mon_part : nullptr;
@@ -572,12 +591,29 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
     return cudaSuccess;
 }
 
+static int run_steps(sddc_ctx *ctx, double dt, int nsteps);
+
 extern "C" int sddc_rk_step(sddc_ctx *ctx, double dt, int nsteps)
 {
     int rc = ready(ctx);
     if (rc) return rc;
+    if (ctx->ncase) return set_err(ctx, SDDC_ESTATE, "a batch steps with sddc_rk_step_cases");
     if (nsteps < 0) return set_err(ctx, SDDC_EINVAL, "nsteps < 0");
     if (!(dt > 0.0)) return set_err(ctx, SDDC_EINVAL, "dt must be positive");
+    return run_steps(ctx, dt, nsteps);
+}
+
+extern "C" int sddc_rk_step_cases(sddc_ctx *ctx, int nsteps)
+{
+    int rc = ready(ctx);
+    if (rc) return rc;
+    if (!ctx->ncase) return set_err(ctx, SDDC_ESTATE, "no batch: call sddc_set_cases first");
+    if (nsteps < 0) return set_err(ctx, SDDC_EINVAL, "nsteps < 0");
+    return run_steps(ctx, 0.0, nsteps);  // each case's dt lives on the device
+}
+
+static int run_steps(sddc_ctx *ctx, double dt, int nsteps)
+{
     for (int s = 0; s < nsteps; s++) {
         const int s0 = ctx->slot;
         cudaGraphExec_t &g = ctx->graph[s0];
@@ -604,7 +640,7 @@ extern "C" int sddc_rk_step(sddc_ctx *ctx, double dt, int nsteps)
             if (e != cudaSuccess) return cuda_err(ctx, e, "stage launch");
         }
         ctx->ctime += dt;  // ctime = ctime0 + dt after the last stage (iterations.f90:211)
-        ctx->mon_nblk = ctx->grid;
+        ctx->mon_nblk = ctx->ncase ? ctx->ntiles_rk : ctx->grid;
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return check_flags(ctx);
@@ -620,6 +656,7 @@ extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *n
     if (resid) CK(cudaMemcpyAsync(resid, ctx->resid, ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (nablaQs)
         CK(cudaMemcpyAsync(nablaQs, ctx->grad, 2 * ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (muAV && ctx->ncase) return set_err(ctx, SDDC_ESTATE, "muAV is per case; read sm_ind for a batch");
     if (muAV) {
         const double h = std::sqrt(ctx->p.dxcycl * ctx->p.dycycl / (double)ctx->p.ncellglob);
         muav_kernel<<<(ctx->ncell + 255) / 256, 256, 0, ctx->stream>>>(ctx->ncell, ctx->N, h, ctx->sm_ind,
@@ -681,5 +718,86 @@ extern "C" int sddc_get_stream(sddc_ctx *ctx, void **stream)
 {
     if (!ctx || !stream) return SDDC_EINVAL;
     *stream = (void *)ctx->stream;
+    return SDDC_OK;
+}
+
+// ---------------------------------------------------------------- batches
+
+static int build_tiles(sddc_ctx *ctx, int cpb, int4 **dev, int *count)
+{
+    std::vector<int4> tiles;
+    for (int c = 0; c < ctx->ncase; c++) {
+        const sddc_case &k = ctx->cases[c];
+        for (int first = 0; first < k.ncell; first += cpb)
+            tiles.push_back(make_int4(k.first_cell + first, std::min(cpb, k.ncell - first), c, first == 0 ? 1 : 0));
+    }
+    cudaFree(*dev);
+    *dev = nullptr;
+    int rc = alloc(ctx, (void **)dev, tiles.size() * sizeof(int4), "tile table");
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(*dev, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+    *count = (int)tiles.size();
+    return SDDC_OK;
+}
+
+extern "C" int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases)
+{
+    if (!ctx || ncase < 1 || !cases) return set_err(ctx, SDDC_EINVAL, "sddc_set_cases: bad arguments");
+    // the cases must tile the cell range in order
+    int next = 0;
+    for (int c = 0; c < ncase; c++) {
+        if (cases[c].first_cell != next || cases[c].ncell < 1)
+            return set_err(ctx, SDDC_EINVAL, "case " + std::to_string(c) + " does not start where the previous ends");
+        if (!(cases[c].dt > 0.0)) return set_err(ctx, SDDC_EINVAL, "case " + std::to_string(c) + ": dt must be positive");
+        next += cases[c].ncell;
+    }
+    if (next != ctx->ncell) return set_err(ctx, SDDC_EINVAL, "the cases do not cover the context's cells");
+    ctx->ncase = ncase;
+    ctx->cases.assign(cases, cases + ncase);
+    std::vector<CaseParams> cp(ncase);
+    for (int c = 0; c < ncase; c++) {
+        const sddc_case &k = cases[c];
+        cp[c].fs = Freestream{k.rinf, k.pinf, k.uinf, k.vinf, k.bxinf, k.byinf};
+        cp[c].dt = k.dt;
+        cp[c].pad = 0.0;
+    }
+    int rc;
+    cudaFree(ctx->case_dev);
+    ctx->case_dev = nullptr;
+    if ((rc = alloc(ctx, (void **)&ctx->case_dev, ncase * sizeof(CaseParams), "case table"))) return rc;
+    CK(cudaMemcpyAsync(ctx->case_dev, cp.data(), ncase * sizeof(CaseParams), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = build_tiles(ctx, ctx->cpb, &ctx->tiles_rk, &ctx->ntiles_rk))) return rc;
+    if ((rc = build_tiles(ctx, 8, &ctx->tiles_diag, &ctx->ntiles_diag))) return rc;
+    // per-case running maxima and per-tile monitor partials
+    cudaFree(ctx->maxima);
+    cudaFree(ctx->mon_part);
+    ctx->maxima = nullptr;
+    ctx->mon_part = nullptr;
+    const int nmon = std::max(ctx->ntiles_rk, ctx->ntiles_diag);
+    if ((rc = alloc(ctx, (void **)&ctx->maxima, (size_t)ncase * kSlots * 2 * sizeof(double), "maxima")) ||
+        (rc = alloc(ctx, (void **)&ctx->mon_part, (size_t)nmon * 2 * sizeof(double), "monitor")))
+        return rc;
+    CK(cudaMemsetAsync(ctx->maxima, 0, (size_t)ncase * kSlots * 2 * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->mon_part, 0, (size_t)nmon * 2 * sizeof(double), ctx->stream));
+    for (auto &g : ctx->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->state = false;  // the maxima were reset: set the state again
+    ctx->mon_nblk = 0;
+    return SDDC_OK;
+}
+
+extern "C" int sddc_get_case_maxima(sddc_ctx *ctx, int icase, double *eigvmax, double *umax)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (icase < 0 || icase >= std::max(ctx->ncase, 1)) return set_err(ctx, SDDC_EINVAL, "case index out of range");
+    CK(cudaMemcpyAsync(ctx->host_small, ctx->maxima + (size_t)icase * kSlots * 2 + 2 * ctx->slot,
+                       2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (eigvmax) *eigvmax = ctx->host_small[0];
+    if (umax) *umax = ctx->host_small[1];
     return SDDC_OK;
 }

@@ -60,6 +60,13 @@ enum RkKind : int {
     kRkFive = 4      // out = ((((c1*a + c2*b) + c3*c) + c4*q) + c5*d) + c0*r   FiveStageRk stage 5
 };
 
+// per-case data of a batch of independent cases sharing one launch
+struct CaseParams {
+    Freestream fs;
+    double dt;
+    double pad;
+};
+
 struct StageArgs {
     int ncell;
     int vismode;
@@ -67,8 +74,18 @@ struct StageArgs {
     int rk_kind;
     int slot_r, slot_w;
     double alpha;
-    double c[8];
-    Freestream fs;
+    // RK coefficients of the stage: c[i] = cb[i] * dt when bit i of dt_mask
+    // is set, else cb[i] (the products round as the host's would)
+    double cb[8];
+    unsigned dt_mask;
+    double dt;                         // single case
+    Freestream fs;                     // single case
+    // batch: one tile per CTA (first cell, cells, case, 1 if the case's
+    // first tile), per-case data and running maxima [case][5][2]; null for
+    // a single case
+    const int4 *tiles;
+    int ntiles;
+    const CaseParams *cases;
     const double *__restrict__ q_in;   // (9,N,N,NCELL), never written during the stage
     double *q_out;                     // RK output (may be reg_a: FiveStageRk stage 5)
     const void *__restrict__ t_in;     // face traces of q_in, R[NCELL][4][N][9]
@@ -198,8 +215,23 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     R *sOpM = sOpL + NP * N;                                     // [NP][N]
 
     const int tid = threadIdx.x;
-    const int c0 = blockIdx.x * CPB;
-    const int ncl = min(CPB, a.ncell - c0);  // cells of this CTA
+    int c0, ncl, cs;
+    bool first_tile;
+    if (a.tiles) {
+        const int4 tl = a.tiles[blockIdx.x];
+        c0 = tl.x;
+        ncl = tl.y;
+        cs = tl.z;
+        first_tile = tl.w != 0;
+    } else {
+        c0 = blockIdx.x * CPB;
+        ncl = min(CPB, a.ncell - c0);  // cells of this CTA
+        cs = 0;
+        first_tile = blockIdx.x == 0;
+    }
+    const Freestream fs = a.cases ? a.cases[cs].fs : a.fs;
+    const double dt = a.cases ? a.cases[cs].dt : a.dt;
+    double *maxima = a.maxima + 10 * cs;
 
     // ---- stage the state, the metrics and the operators ------------------------
     for (int k = tid; k < NP * N; k += NT) {
@@ -223,7 +255,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
         }
     }
-    const double eig_r = a.maxima[2 * a.slot_r], um_r = a.maxima[2 * a.slot_r + 1];
+    const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
     const R c_h = (R)sqrt(eig_r * (eig_r - um_r));
     __syncthreads();
@@ -313,7 +345,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             n0 = onrm[0]; n1 = onrm[1];
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
-            bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.fs, other);
+            bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, fs, other);
         }
         // left and right states by element-wise selects (arrays picked
         // through a pointer would live in local memory)
@@ -560,7 +592,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         if constexpr (DIAG) {
             for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sRes[e];
         } else {
-            const double *cf = a.c;
+            double cf[6];
+#pragma unroll
+            for (int i = 0; i < 6; i++) cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
             for (int e = tid; e < n; e += NT) {
                 const size_t g = g0 + e;
                 const double q = sQ[e], r = sRes[e];
@@ -633,11 +667,11 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 s0 += sRed[64 + w];
                 s1 += sRed[96 + w];
             }
-            atomic_max_nonneg(&a.maxima[2 * a.slot_w], m0);
-            atomic_max_nonneg(&a.maxima[2 * a.slot_w + 1], m1);
-            if (blockIdx.x == 0) {  // carry the previous stages' maxima forward
-                atomic_max_nonneg(&a.maxima[2 * a.slot_w], eig_r);
-                atomic_max_nonneg(&a.maxima[2 * a.slot_w + 1], um_r);
+            atomic_max_nonneg(&maxima[2 * a.slot_w], m0);
+            atomic_max_nonneg(&maxima[2 * a.slot_w + 1], m1);
+            if (first_tile) {  // carry the previous stages' maxima forward
+                atomic_max_nonneg(&maxima[2 * a.slot_w], eig_r);
+                atomic_max_nonneg(&maxima[2 * a.slot_w + 1], um_r);
             }
             if (a.mon_part) {
                 a.mon_part[2 * blockIdx.x] = s0;

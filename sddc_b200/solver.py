@@ -31,7 +31,8 @@ OK, EINVAL, ECUDA, ESTATE, ENUMERIC, ENOMEM = 0, -1, -2, -3, -4, -5
 
 EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables", "sddc_set_state",
             "sddc_compresid", "sddc_rk_step", "sddc_get_state", "sddc_monitor", "sddc_get_maxima",
-            "sddc_state_device_ptr", "sddc_get_stream")
+            "sddc_state_device_ptr", "sddc_get_stream", "sddc_set_cases", "sddc_rk_step_cases",
+            "sddc_get_case_maxima")
 
 
 class Params(ctypes.Structure):
@@ -39,6 +40,12 @@ class Params(ctypes.Structure):
                 ("precision", _I), ("cells_per_cta", _I), ("mu", _D), ("eta0", _D), ("dxcycl", _D),
                 ("dycycl", _D), ("rinf", _D), ("pinf", _D), ("uinf", _D), ("vinf", _D), ("bxinf", _D),
                 ("byinf", _D)]
+
+
+class CaseRecord(ctypes.Structure):
+    """sddc_case: one case of a batch."""
+    _fields_ = [("first_cell", _I), ("ncell", _I), ("dt", _D), ("rinf", _D), ("pinf", _D), ("uinf", _D),
+                ("vinf", _D), ("bxinf", _D), ("byinf", _D)]
 
 
 class SddcError(RuntimeError):
@@ -68,6 +75,9 @@ def lib():
         L.sddc_get_maxima.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD]
         L.sddc_state_device_ptr.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         L.sddc_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.sddc_set_cases.argtypes = [ctypes.c_void_p, _I, ctypes.POINTER(CaseRecord)]
+        L.sddc_rk_step_cases.argtypes = [ctypes.c_void_p, _I]
+        L.sddc_get_case_maxima.argtypes = [ctypes.c_void_p, _I, _PD, _PD]
         L._sddc_typed = True
     return L
 
@@ -190,6 +200,25 @@ class Solver:
         p = ctypes.c_void_p()
         self._check(self._L.sddc_get_stream(self._h, ctypes.byref(p)))
         return p.value
+
+    # -- batches of cases ---------------------------------------------------
+    def set_cases(self, records):
+        """records: sequence of dicts with first_cell, ncell, dt and the free
+        stream (rinf, pinf, uinf, vinf, bxinf, byinf)."""
+        arr = (CaseRecord * len(records))()
+        for k, r in enumerate(records):
+            for f, _ in CaseRecord._fields_:
+                setattr(arr[k], f, r[f])
+        self._check(self._L.sddc_set_cases(self._h, len(records), arr))
+        self.ncase = len(records)
+
+    def step_cases(self, nsteps=1):
+        self._check(self._L.sddc_rk_step_cases(self._h, int(nsteps)))
+
+    def case_maxima(self, icase):
+        e, u = _D(), _D()
+        self._check(self._L.sddc_get_case_maxima(self._h, int(icase), ctypes.byref(e), ctypes.byref(u)))
+        return e.value, u.value
 
     # -- the reference's time loop -------------------------------------------
     def iterations(self, dt, maxiter, resid_out=None, iter0=0, ncellglob=None):
