@@ -229,8 +229,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         cs = 0;
         first_tile = blockIdx.x == 0;
     }
-    const Freestream fs = a.cases ? a.cases[cs].fs : a.fs;
-    const double dt = a.cases ? a.cases[cs].dt : a.dt;
+    // per-case data is read where it is used (kept out of registers)
     double *maxima = a.maxima + 10 * cs;
 
     // ---- stage the state, the metrics and the operators ------------------------
@@ -345,7 +344,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             n0 = onrm[0]; n1 = onrm[1];
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
-            bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, fs, other);
+            bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.cases ? a.cases[cs].fs : a.fs, other);
         }
         // left and right states by element-wise selects (arrays picked
         // through a pointer would live in local memory)
@@ -594,7 +593,10 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         } else {
             double cf[6];
 #pragma unroll
-            for (int i = 0; i < 6; i++) cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
+            for (int i = 0; i < 6; i++) {
+                const double dt = a.cases ? a.cases[cs].dt : a.dt;
+                cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
+            }
             for (int e = tid; e < n; e += NT) {
                 const size_t g = g0 + e;
                 const double q = sQ[e], r = sRes[e];
