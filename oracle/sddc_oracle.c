@@ -26,6 +26,26 @@
 
 #define NV 9
 
+typedef orc_real real;
+
+/* Arithmetic type of every state-dependent quantity.  The plain build uses
+ * double.  The tangent build (-DORC_CSTEP) uses double _Complex: a state
+ * Q + i*h*V evaluated with h ~ 1e-30 carries Im(f)/h = f'(Q).V to rounding
+ * (complex-step differentiation, Squire & Trapp 1998).  Branches, |x| and
+ * max() follow the real part, so the tangent is that of the branch the
+ * plain build takes. */
+#ifdef ORC_CSTEP
+#define RV(x) creal(x)
+static inline real r_sqrt(real x) { return csqrt(x); }
+static inline real r_abs(real x) { return creal(x) < 0.0 ? -x : x; }
+static inline real r_max(real a, real b) { return creal(b) > creal(a) ? b : a; }
+#else
+#define RV(x) (x)
+#define r_sqrt sqrt
+#define r_abs fabs
+#define r_max fmax
+#endif
+
 struct orc_ctx {
     orc_params p;
     int N, N1, NC;
@@ -40,11 +60,15 @@ struct orc_ctx {
         *cyc2fpair;
     int iface2fp[4 * 16], jface2fp[4 * 16]; /* (nfp,lf), N <= 16 */
     /* state and work arrays */
-    double *Q, *resid, *F1, *G2, *Fv1, *Gv2, *Qvfi, *Qvfj;
-    double *nablaQs, *nablaQvfi, *nablaQvfj, *dedxi, *dedeta;
+    real *Q, *resid, *F1, *G2, *Fv1, *Gv2, *Qvfi, *Qvfj;
+    real *nablaQs, *nablaQvfi, *nablaQvfj, *dedxi, *dedeta;
     double *muAV, *SM_IND, *muAVfi, *muAVfj;
+    /* free stream of the boundary states (rinf, pinf, uinf, vinf, bxinf,
+       byinf), a copy of the parameters that the tangent build can perturb */
+    real fs[6];
     /* scalars of module setup2d */
-    double eigvmax, eigvmax_g, umax, umax_g, c_h, epsilon0, ctime;
+    real eigvmax, eigvmax_g, umax, umax_g, c_h;
+    double epsilon0, ctime;
 };
 
 /* ---- accessors (1-based, Fortran column-major) ----------------------- */
@@ -76,8 +100,8 @@ static const double GAM = 5.0 / 3.0;        /* setup2d.f90:67 */
 static const double LAMBDA = -2.0 / 3.0;    /* setup2d.f90:69 */
 static const double PRANDT = 0.72;          /* setup2d.f90:70 */
 
-static inline double sq(double x) { return x * x; }
-static inline void upd_max(double *m, double x) { if (x > *m) *m = x; }
+static inline real sq(real x) { return x * x; }
+static inline void upd_max(real *m, real x) { if (RV(x) > RV(*m)) *m = x; }
 
 /* ===================================================================== */
 /* SD points and operators                                               */
@@ -263,6 +287,8 @@ orc_ctx *orc_create(const orc_params *p)
     long NC = p->ncell;
     cx->N = N; cx->N1 = N1; cx->NC = (int)NC;
     cx->alpha = 2.0; /* initsetup.f90:165 */
+    cx->fs[0] = p->rinf; cx->fs[1] = p->pinf; cx->fs[2] = p->uinf;
+    cx->fs[3] = p->vinf; cx->fs[4] = p->bxinf; cx->fs[5] = p->byinf;
     cx->Xs = zalloc(sizeof(double) * N);
     cx->Xf = zalloc(sizeof(double) * N1);
     cx->Lmat = zalloc(sizeof(double) * N1 * N);
@@ -277,19 +303,19 @@ orc_ctx *orc_create(const orc_params *p)
     cx->S1 = zalloc(sizeof(double) * 4 * nfi);
     cx->S2 = zalloc(sizeof(double) * 4 * nfi);
     cx->Jac = zalloc(sizeof(double) * nsp);
-    cx->Q = zalloc(sizeof(double) * NV * nsp);
-    cx->resid = zalloc(sizeof(double) * NV * nsp);
-    cx->F1 = zalloc(sizeof(double) * NV * nfi);
-    cx->G2 = zalloc(sizeof(double) * NV * nfi);
-    cx->Fv1 = zalloc(sizeof(double) * NV * nfi);
-    cx->Gv2 = zalloc(sizeof(double) * NV * nfi);
-    cx->Qvfi = zalloc(sizeof(double) * NV * nfi);
-    cx->Qvfj = zalloc(sizeof(double) * NV * nfi);
-    cx->nablaQs = zalloc(sizeof(double) * NV * 2 * nsp);
-    cx->nablaQvfi = zalloc(sizeof(double) * NV * 2 * nfi);
-    cx->nablaQvfj = zalloc(sizeof(double) * NV * 2 * nfi);
-    cx->dedxi = zalloc(sizeof(double) * nsp);
-    cx->dedeta = zalloc(sizeof(double) * nsp);
+    cx->Q = zalloc(sizeof(real) * NV * nsp);
+    cx->resid = zalloc(sizeof(real) * NV * nsp);
+    cx->F1 = zalloc(sizeof(real) * NV * nfi);
+    cx->G2 = zalloc(sizeof(real) * NV * nfi);
+    cx->Fv1 = zalloc(sizeof(real) * NV * nfi);
+    cx->Gv2 = zalloc(sizeof(real) * NV * nfi);
+    cx->Qvfi = zalloc(sizeof(real) * NV * nfi);
+    cx->Qvfj = zalloc(sizeof(real) * NV * nfi);
+    cx->nablaQs = zalloc(sizeof(real) * NV * 2 * nsp);
+    cx->nablaQvfi = zalloc(sizeof(real) * NV * 2 * nfi);
+    cx->nablaQvfj = zalloc(sizeof(real) * NV * 2 * nfi);
+    cx->dedxi = zalloc(sizeof(real) * nsp);
+    cx->dedeta = zalloc(sizeof(real) * nsp);
     cx->muAV = zalloc(sizeof(double) * 2 * NC);
     cx->SM_IND = zalloc(sizeof(double) * 2 * NC);
     cx->muAVfi = zalloc(sizeof(double) * 4 * NC);
@@ -354,10 +380,10 @@ int orc_set_tables(orc_ctx *cx, const double *Lmat, const double *Mmat,
     return 0;
 }
 
-void orc_set_state(orc_ctx *cx, const double *Q, double ctime,
+void orc_set_state(orc_ctx *cx, const real *Q, double ctime,
                    double eigvmax, double umax)
 {
-    memcpy(cx->Q, Q, sizeof(double) * NV * cx->N * cx->N * (long)cx->NC);
+    memcpy(cx->Q, Q, sizeof(real) * NV * cx->N * cx->N * (long)cx->NC);
     cx->ctime = ctime;
     /* initsetup.f90:166-167 sets the local maxima; the global copies are
        zero-initialised module scalars until the first allreduce. */
@@ -367,13 +393,13 @@ void orc_set_state(orc_ctx *cx, const double *Q, double ctime,
     cx->umax_g = umax;
 }
 
-void orc_get_state(const orc_ctx *cx, double *Q, double *resid,
-                   double *nablaQs, double *muAV, double *sm_ind)
+void orc_get_state(const orc_ctx *cx, real *Q, real *resid,
+                   real *nablaQs, double *muAV, double *sm_ind)
 {
     long nsp = (long)cx->N * cx->N * cx->NC;
-    if (Q) memcpy(Q, cx->Q, sizeof(double) * NV * nsp);
-    if (resid) memcpy(resid, cx->resid, sizeof(double) * NV * nsp);
-    if (nablaQs) memcpy(nablaQs, cx->nablaQs, sizeof(double) * NV * 2 * nsp);
+    if (Q) memcpy(Q, cx->Q, sizeof(real) * NV * nsp);
+    if (resid) memcpy(resid, cx->resid, sizeof(real) * NV * nsp);
+    if (nablaQs) memcpy(nablaQs, cx->nablaQs, sizeof(real) * NV * 2 * nsp);
     if (muAV) memcpy(muAV, cx->muAV, sizeof(double) * 2 * cx->NC);
     if (sm_ind) memcpy(sm_ind, cx->SM_IND, sizeof(double) * 2 * cx->NC);
 }
@@ -381,21 +407,26 @@ void orc_get_state(const orc_ctx *cx, double *Q, double *resid,
 void orc_get_maxima(const orc_ctx *cx, double *eigvmax, double *umax,
                     double *c_h, double *epsilon0, double *ctime)
 {
-    if (eigvmax) *eigvmax = cx->eigvmax_g;
-    if (umax) *umax = cx->umax_g;
-    if (c_h) *c_h = cx->c_h;
+    if (eigvmax) *eigvmax = RV(cx->eigvmax_g);
+    if (umax) *umax = RV(cx->umax_g);
+    if (c_h) *c_h = RV(cx->c_h);
     if (epsilon0) *epsilon0 = cx->epsilon0;
     if (ctime) *ctime = cx->ctime;
 }
 
-void orc_get_fluxes(const orc_ctx *cx, double *F1, double *G2, double *Fv1,
-                    double *Gv2)
+void orc_get_fluxes(const orc_ctx *cx, real *F1, real *G2, real *Fv1,
+                    real *Gv2)
 {
     long nfi = (long)cx->N1 * cx->N * cx->NC * NV;
-    if (F1) memcpy(F1, cx->F1, sizeof(double) * nfi);
-    if (G2) memcpy(G2, cx->G2, sizeof(double) * nfi);
-    if (Fv1) memcpy(Fv1, cx->Fv1, sizeof(double) * nfi);
-    if (Gv2) memcpy(Gv2, cx->Gv2, sizeof(double) * nfi);
+    if (F1) memcpy(F1, cx->F1, sizeof(real) * nfi);
+    if (G2) memcpy(G2, cx->G2, sizeof(real) * nfi);
+    if (Fv1) memcpy(Fv1, cx->Fv1, sizeof(real) * nfi);
+    if (Gv2) memcpy(Gv2, cx->Gv2, sizeof(real) * nfi);
+}
+
+void orc_set_freestream(orc_ctx *cx, const real *fs)
+{
+    for (int k = 0; k < 6; k++) cx->fs[k] = fs[k];
 }
 
 /* ===================================================================== */
@@ -403,13 +434,13 @@ void orc_get_fluxes(const orc_ctx *cx, double *F1, double *G2, double *Fv1,
 /* ===================================================================== */
 
 /* getIfluxvectors, getrusanov.f90:127-193 */
-static void iflux(const double *Qi, double c_h, double *umax, double *Fi,
-                  double *Gi)
+static void iflux(const real *Qi, real c_h, real *umax, real *Fi,
+                  real *Gi)
 {
-    double rho = Qi[0], rhou = Qi[1], rhov = Qi[2], rhow = Qi[3],
+    real rho = Qi[0], rhou = Qi[1], rhov = Qi[2], rhow = Qi[3],
            rhoE = Qi[4], Bx = Qi[5], By = Qi[6], Bz = Qi[7], psi = Qi[8];
-    double NORM_B = (Bx * Bx + By * By) + Bz * Bz;
-    double pr = (GAM - 1.0) * (((rhoE - 0.5 * ((rhou * rhou + rhov * rhov) + rhow * rhow) / rho)
+    real NORM_B = (Bx * Bx + By * By) + Bz * Bz;
+    real pr = (GAM - 1.0) * (((rhoE - 0.5 * ((rhou * rhou + rhov * rhov) + rhow * rhow) / rho)
                                 - 0.5 * NORM_B) - 0.5 * (psi * psi));
     Fi[0] = rhou;
     Fi[1] = ((rhou * rhou) / rho + pr) + (0.5 * NORM_B - Bx * Bx);
@@ -438,46 +469,46 @@ static void iflux(const double *Qi, double c_h, double *umax, double *Fi,
     Fi[8] = c_h * Bx;
     Gi[8] = c_h * By;
 
-    double u = rhou / rho, v = rhov / rho, w = rhow / rho;
-    double umaxtmp = fmax(fmax(fabs(u), fabs(v)), fabs(w));
+    real u = rhou / rho, v = rhov / rho, w = rhow / rho;
+    real umaxtmp = r_max(r_max(r_abs(u), r_abs(v)), r_abs(w));
     upd_max(umax, umaxtmp);
 }
 
-void orc_point_iflux(const double *Qi, double c_h, double *umax, double *F,
-                     double *G)
+void orc_point_iflux(const real *Qi, real c_h, real *umax, real *F,
+                     real *G)
 {
     iflux(Qi, c_h, umax, F, G);
 }
 
 /* getrusanovflux, getrusanov.f90:1-125 */
-static void rusanov(const double *Qfl, const double *Qfr, double *Fnl,
-                    double *Fnr, const double *normf, int sign_l, int sign_r,
-                    double c_h, double *eigv_out, double *eigvmax,
-                    double *umax)
+static void rusanov(const real *Qfl, const real *Qfr, real *Fnl,
+                    real *Fnr, const real *normf, int sign_l, int sign_r,
+                    real c_h, real *eigv_out, real *eigvmax,
+                    real *umax)
 {
-    double magnorm = sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
-    double unit_x = normf[0] / magnorm * (double)sign_l;
-    double unit_y = normf[1] / magnorm * (double)sign_l;
+    real magnorm = r_sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
+    real unit_x = normf[0] / magnorm * (real)sign_l;
+    real unit_y = normf[1] / magnorm * (real)sign_l;
 
-    double rhoi = 1.0 / Qfl[0];
-    double ul = rhoi * Qfl[1], vl = rhoi * Qfl[2], wl = rhoi * Qfl[3];
-    double Bxl = Qfl[5], Byl = Qfl[6], Bzl = Qfl[7], psil = Qfl[8];
-    double NORM_Bl = (Bxl * Bxl + Byl * Byl) + Bzl * Bzl;
-    double pl = (GAM - 1.0) * (((Qfl[4] - 0.5 * Qfl[0] * ((ul * ul + vl * vl) + wl * wl))
+    real rhoi = 1.0 / Qfl[0];
+    real ul = rhoi * Qfl[1], vl = rhoi * Qfl[2], wl = rhoi * Qfl[3];
+    real Bxl = Qfl[5], Byl = Qfl[6], Bzl = Qfl[7], psil = Qfl[8];
+    real NORM_Bl = (Bxl * Bxl + Byl * Byl) + Bzl * Bzl;
+    real pl = (GAM - 1.0) * (((Qfl[4] - 0.5 * Qfl[0] * ((ul * ul + vl * vl) + wl * wl))
                                 - NORM_Bl * 0.5) - 0.5 * (psil * psil));
     pl = pl + 0.5 * NORM_Bl;
-    double Vn_l = ul * unit_x + vl * unit_y;
-    double Bn_l = Bxl * unit_x + Byl * unit_y;
+    real Vn_l = ul * unit_x + vl * unit_y;
+    real Bn_l = Bxl * unit_x + Byl * unit_y;
 
     rhoi = 1.0 / Qfr[0];
-    double ur = rhoi * Qfr[1], vr = rhoi * Qfr[2], wr = rhoi * Qfr[3];
-    double Bxr = Qfr[5], Byr = Qfr[6], Bzr = Qfr[7], psir = Qfr[8];
-    double NORM_Br = (Bxr * Bxr + Byr * Byr) + Bzr * Bzr;
-    double pr = (GAM - 1.0) * (((Qfr[4] - 0.5 * Qfr[0] * ((ur * ur + vr * vr) + wr * wr))
+    real ur = rhoi * Qfr[1], vr = rhoi * Qfr[2], wr = rhoi * Qfr[3];
+    real Bxr = Qfr[5], Byr = Qfr[6], Bzr = Qfr[7], psir = Qfr[8];
+    real NORM_Br = (Bxr * Bxr + Byr * Byr) + Bzr * Bzr;
+    real pr = (GAM - 1.0) * (((Qfr[4] - 0.5 * Qfr[0] * ((ur * ur + vr * vr) + wr * wr))
                                 - NORM_Br * 0.5) - 0.5 * (psir * psir));
     pr = pr + NORM_Br * 0.5;
-    double Vn_r = ur * unit_x + vr * unit_y;
-    double Bn_r = Bxr * unit_x + Byr * unit_y;
+    real Vn_r = ur * unit_x + vr * unit_y;
+    real Bn_r = Bxr * unit_x + Byr * unit_y;
 
     Fnl[0] = Qfl[0] * Vn_l;
     Fnl[1] = (Qfl[1] * Vn_l + pl * unit_x) - Bxl * Bn_l;
@@ -510,33 +541,33 @@ static void rusanov(const double *Qfl, const double *Qfr, double *Fnl,
 
     pl = pl - 0.5 * NORM_Bl;
     pr = pr - 0.5 * NORM_Br;
-    double Bx = 0.5 * (Bxl + Bxr), By = 0.5 * (Byl + Byr), Bz = 0.5 * (Bzl + Bzr);
-    double c_a = GAM * (pl + pr) / (Qfl[0] + Qfr[0]);
-    double c_d = ((Bx * Bx + By * By) + Bz * Bz) / (0.5 * (Qfl[0] + Qfr[0]));
-    double bn = Bx * unit_x + By * unit_y;
-    double c_n = bn * bn / (0.5 * (Qfl[0] + Qfr[0]));
-    double cad = c_a + c_d;
-    double c_tmp = sqrt(cad * cad - 4.0 * c_a * c_n);
-    double c_f = sqrt(0.5 * ((c_a + c_d) + c_tmp));
-    double eigv = 0.5 * fabs(Vn_l + Vn_r) + c_f;
+    real Bx = 0.5 * (Bxl + Bxr), By = 0.5 * (Byl + Byr), Bz = 0.5 * (Bzl + Bzr);
+    real c_a = GAM * (pl + pr) / (Qfl[0] + Qfr[0]);
+    real c_d = ((Bx * Bx + By * By) + Bz * Bz) / (0.5 * (Qfl[0] + Qfr[0]));
+    real bn = Bx * unit_x + By * unit_y;
+    real c_n = bn * bn / (0.5 * (Qfl[0] + Qfr[0]));
+    real cad = c_a + c_d;
+    real c_tmp = r_sqrt(cad * cad - 4.0 * c_a * c_n);
+    real c_f = r_sqrt(0.5 * ((c_a + c_d) + c_tmp));
+    real eigv = 0.5 * r_abs(Vn_l + Vn_r) + c_f;
 
     for (int k = 0; k < NV; k++)
         Fnl[k] = 0.5 * ((Fnl[k] + Fnr[k]) - eigv * (Qfr[k] - Qfl[k]));
-    double sl = magnorm * (double)sign_l;
+    real sl = magnorm * (real)sign_l;
     for (int k = 0; k < NV; k++) Fnl[k] = sl * Fnl[k];
-    double slr = (double)(sign_l * sign_r);
+    real slr = (real)(sign_l * sign_r);
     for (int k = 0; k < NV; k++) Fnr[k] = slr * Fnl[k];
 
     upd_max(eigvmax, eigv);
-    double umaxtmp = fmax(fmax(0.5 * fabs(ul + ur), 0.5 * fabs(vl + vr)), 0.5 * fabs(wl + wr));
+    real umaxtmp = r_max(r_max(0.5 * r_abs(ul + ur), 0.5 * r_abs(vl + vr)), 0.5 * r_abs(wl + wr));
     upd_max(umax, umaxtmp);
     if (eigv_out) *eigv_out = eigv;
 }
 
-void orc_point_rusanov(const double *Qfl, const double *Qfr, double *Fnl,
-                       double *Fnr, const double *normf, int sign_l,
-                       int sign_r, double c_h, double *eigv,
-                       double *eigvmax, double *umax)
+void orc_point_rusanov(const real *Qfl, const real *Qfr, real *Fnl,
+                       real *Fnr, const real *normf, int sign_l,
+                       int sign_r, real c_h, real *eigv,
+                       real *eigvmax, real *umax)
 {
     rusanov(Qfl, Qfr, Fnl, Fnr, normf, sign_l, sign_r, c_h, eigv, eigvmax, umax);
 }
@@ -544,16 +575,16 @@ void orc_point_rusanov(const double *Qfl, const double *Qfr, double *Fnl,
 /* getVfluxvectors (getrusanov.f90:197-294) with viscosity mu and
    resistivity eta; getVfluxvectors_AV (:296-413) is the same formula with
    its hard-coded mu_art = eta_art = 0 (:326, :328). */
-static void vflux(const double *Qv, const double *nQ /* (9,2) */, double mu,
-                  double eta0, double *Fv, double *Gv)
+static void vflux(const real *Qv, const real *nQ /* (9,2) */, real mu,
+                  real eta0, real *Fv, real *Gv)
 {
-    double rho = Qv[0], rhou = Qv[1], rhov = Qv[2], rhow = Qv[3],
+    real rho = Qv[0], rhou = Qv[1], rhov = Qv[2], rhow = Qv[3],
            rhoE = Qv[4], Bx = Qv[5], By = Qv[6], Bz = Qv[7], psi = Qv[8];
-    double u = rhou / rho, v = rhov / rho, w = rhow / rho;
-    double NORM_U = (u * u + v * v) + w * w;
-    double NORM_B = (Bx * Bx + By * By) + Bz * Bz;
-    double inte = (((rhoE - 0.5 * NORM_U * rho) - 0.5 * NORM_B) - 0.5 * (psi * psi)) / rho;
-    double drho[2], du[2], dv[2], dw[2], dBx[2], dBy[2], dBz[2], dpsi[2],
+    real u = rhou / rho, v = rhov / rho, w = rhow / rho;
+    real NORM_U = (u * u + v * v) + w * w;
+    real NORM_B = (Bx * Bx + By * By) + Bz * Bz;
+    real inte = (((rhoE - 0.5 * NORM_U * rho) - 0.5 * NORM_B) - 0.5 * (psi * psi)) / rho;
+    real drho[2], du[2], dv[2], dw[2], dBx[2], dBy[2], dBz[2], dpsi[2],
         dKE[2], dpre_B[2], dpsi2[2], de[2];
     for (int d = 0; d < 2; d++) {
         drho[d] = nQ[0 + NV * d];
@@ -569,9 +600,9 @@ static void vflux(const double *Qv, const double *nQ /* (9,2) */, double mu,
         dpsi2[d] = psi * dpsi[d];
         de[d] = ((((nQ[4 + NV * d] - dKE[d]) - dpre_B[d]) - drho[d] * inte) - dpsi2[d]) / rho;
     }
-    double ux = du[0], uy = du[1], vx = dv[0], vy = dv[1], wx = dw[0],
+    real ux = du[0], uy = du[1], vx = dv[0], vy = dv[1], wx = dw[0],
            wy = dw[1], ex = de[0], ey = de[1];
-    double Bxy = dBx[1], Byx = dBy[0], Bzx = dBz[0], Bzy = dBz[1];
+    real Bxy = dBx[1], Byx = dBy[0], Bzx = dBz[0], Bzy = dBz[1];
 
     Fv[0] = 0.0;
     Fv[1] = mu * (2.0 * ux + LAMBDA * (ux + vy));
@@ -584,7 +615,7 @@ static void vflux(const double *Qv, const double *nQ /* (9,2) */, double mu,
     Gv[3] = mu * wy;
     Gv[4] = ((Gv[1] * u + Gv[2] * v) + Gv[3] * w) + mu * GAM * ey / PRANDT;
 
-    double Jx = Bzy - 0.0, Jy = 0.0 - Bzx, Jz = Byx - Bxy;
+    real Jx = Bzy - 0.0, Jy = 0.0 - Bzx, Jz = Byx - Bxy;
     Fv[5] = 0.0;
     Fv[6] = eta0 * Jz;
     Fv[7] = -(eta0 * Jy);
@@ -604,7 +635,7 @@ static void vflux(const double *Qv, const double *nQ /* (9,2) */, double mu,
 /* Interpolate Q to the flux point of local face lf, face point nfp
    (the left/right blocks of interfaceflux_all.f90:35-77). */
 static void face_trace(const orc_ctx *cx, int ic, int lf, int nfp,
-                       double *Qf, int *ifp_o, int *jfp_o)
+                       real *Qf, int *ifp_o, int *jfp_o)
 {
     int N = cx->N, N1 = cx->N1;
     int ifp = IFP_(nfp, lf), jfp = JFP_(nfp, lf);
@@ -624,7 +655,7 @@ static void face_trace(const orc_ctx *cx, int ic, int lf, int nfp,
 }
 
 static void face_normal(const orc_ctx *cx, int ic, int lf, int ifp, int jfp,
-                        double *normf)
+                        real *normf)
 {
     int N = cx->N, N1 = cx->N1;
     if ((lf % 2) + 1 == 1) {
@@ -636,8 +667,8 @@ static void face_normal(const orc_ctx *cx, int ic, int lf, int ifp, int jfp,
     }
 }
 
-static void store_face(orc_ctx *cx, double *Ai, double *Aj, int ic, int lf,
-                       int ifp, int jfp, const double *val)
+static void store_face(orc_ctx *cx, real *Ai, real *Aj, int ic, int lf,
+                       int ifp, int jfp, const real *val)
 {
     int N = cx->N, N1 = cx->N1;
     if ((lf % 2) + 1 == 1) {
@@ -653,15 +684,15 @@ static void store_face(orc_ctx *cx, double *Ai, double *Aj, int ic, int lf,
 static void inviscid_flux_interior(orc_ctx *cx)
 {
     int N = cx->N, N1 = cx->N1, NC = cx->NC;
-    double umax_all = cx->umax;
+    real umax_all = cx->umax;
     int vis = cx->p.vismode;
-    double c_h = cx->c_h;
+    real c_h = cx->c_h;
 #pragma omp parallel
     {
-        double um = cx->umax;
+        real um = cx->umax;
 #pragma omp for schedule(static)
         for (int ic = 1; ic <= NC; ic++) {
-            double Qf[NV], F[NV], G[NV];
+            real Qf[NV], F[NV], G[NV];
             for (int jfp = 1; jfp <= N; jfp++)
                 for (int ifp = 2; ifp <= N; ifp++) {
                     for (int k = 0; k < NV; k++) Qf[k] = 0.0;
@@ -671,7 +702,7 @@ static void inviscid_flux_interior(orc_ctx *cx)
                     if (vis == 1)
                         for (int k = 1; k <= NV; k++) FI_(Qvfi, k, ifp, jfp, ic) = Qf[k - 1];
                     iflux(Qf, c_h, &um, F, G);
-                    double s11 = S1_(1, 1, ifp, jfp, ic), s12 = S1_(1, 2, ifp, jfp, ic);
+                    real s11 = S1_(1, 1, ifp, jfp, ic), s12 = S1_(1, 2, ifp, jfp, ic);
                     for (int k = 1; k <= NV; k++)
                         FI_(F1, k, ifp, jfp, ic) = F[k - 1] * s11 + G[k - 1] * s12;
                 }
@@ -684,7 +715,7 @@ static void inviscid_flux_interior(orc_ctx *cx)
                     if (vis == 1)
                         for (int k = 1; k <= NV; k++) FJ_(Qvfj, k, ifp, jfp, ic) = Qf[k - 1];
                     iflux(Qf, c_h, &um, F, G);
-                    double s21 = S2_(2, 1, ifp, jfp, ic), s22 = S2_(2, 2, ifp, jfp, ic);
+                    real s21 = S2_(2, 1, ifp, jfp, ic), s22 = S2_(2, 2, ifp, jfp, ic);
                     for (int k = 1; k <= NV; k++)
                         FJ_(G2, k, ifp, jfp, ic) = F[k - 1] * s21 + G[k - 1] * s22;
                 }
@@ -698,10 +729,10 @@ static void inviscid_flux_interior(orc_ctx *cx)
 /* One face shared by two cells: interfaceflux (interfaceflux_all.f90:16-110)
    and CYCLOCFLUX (cyclocflux_all.f90:15-110) run the same body. */
 static void pair_flux(orc_ctx *cx, int icleft, int icright, int ifacelc,
-                      int ifacerc, double *em, double *um)
+                      int ifacerc, real *em, real *um)
 {
     int N = cx->N;
-    double Qfl[NV], Qfr[NV], Fnl[NV], Fnr[NV], normf[2], avg[NV], eigv;
+    real Qfl[NV], Qfr[NV], Fnl[NV], Fnr[NV], normf[2], avg[NV], eigv;
     for (int nfp = 1; nfp <= N; nfp++) {
         int ifpl, jfpl, ifpr, jfpr;
         face_trace(cx, icleft, ifacelc, nfp, Qfl, &ifpl, &jfpl);
@@ -728,10 +759,10 @@ static void pair_flux(orc_ctx *cx, int icleft, int icright, int ifacelc,
 
 static void interface_and_cyclic_flux(orc_ctx *cx)
 {
-    double em_all = cx->eigvmax, um_all = cx->umax;
+    real em_all = cx->eigvmax, um_all = cx->umax;
 #pragma omp parallel
     {
-        double em = cx->eigvmax, um = cx->umax;
+        real em = cx->eigvmax, um = cx->umax;
 #pragma omp for schedule(static)
         for (int f = 1; f <= cx->ninter; f++) {
             int iface = cx->ibfinter[f - 1];
@@ -757,39 +788,39 @@ static void interface_and_cyclic_flux(orc_ctx *cx)
 enum { BC_INLE = 0, BC_OUTL, BC_WALL, BC_SYMP, BC_FREE };
 
 /* Ghost state of one boundary flux point, BCFLUX (bcflux.f90:1-377). */
-static void bc_ghost(const orc_ctx *cx, int kind, const double *Qfl,
-                     const double *normf, double *Qfr)
+static void bc_ghost(const orc_ctx *cx, int kind, const real *Qfl,
+                     const real *normf, real *Qfr)
 {
     const orc_params *p = &cx->p;
     if (kind == BC_INLE) { /* bcflux.f90:51-72 */
-        double rhor = p->rinf, ur = p->uinf, vr = p->vinf, wr = 0.0;
-        double Bxr = p->bxinf, Byr = p->byinf, Bzr = 0.0;
+        real rhor = cx->fs[0], ur = cx->fs[2], vr = cx->fs[3], wr = 0.0;
+        real Bxr = cx->fs[4], Byr = cx->fs[5], Bzr = 0.0;
         Qfr[0] = rhor;
         Qfr[1] = rhor * ur;
         Qfr[2] = rhor * vr;
         Qfr[3] = rhor * wr;
-        Qfr[4] = ((p->pinf / (GAM - 1.0) + 0.5 * rhor * ((ur * ur + vr * vr) + wr * wr))
+        Qfr[4] = ((cx->fs[1] / (GAM - 1.0) + 0.5 * rhor * ((ur * ur + vr * vr) + wr * wr))
                   + 0.5 * ((Bxr * Bxr + Byr * Byr) + Bzr * Bzr)) + 0.5 * (Qfl[8] * Qfl[8]);
         Qfr[5] = Bxr;
         Qfr[6] = Byr;
         Qfr[7] = Bzr;
         Qfr[8] = Qfl[8];
     } else if (kind == BC_OUTL) { /* :122-143 */
-        double rhor = Qfl[0], ur = Qfl[1] / Qfl[0], vr = Qfl[2] / Qfl[0], wr = 0.0;
-        double Bxr = p->bxinf, Byr = p->byinf, Bzr = 0.0;
+        real rhor = Qfl[0], ur = Qfl[1] / Qfl[0], vr = Qfl[2] / Qfl[0], wr = 0.0;
+        real Bxr = cx->fs[4], Byr = cx->fs[5], Bzr = 0.0;
         Qfr[0] = rhor;
         Qfr[1] = rhor * ur;
         Qfr[2] = rhor * vr;
         Qfr[3] = rhor * wr;
-        Qfr[4] = ((p->pinf / (GAM - 1.0) + 0.5 * rhor * ((ur * ur + vr * vr) + wr * wr))
+        Qfr[4] = ((cx->fs[1] / (GAM - 1.0) + 0.5 * rhor * ((ur * ur + vr * vr) + wr * wr))
                   + 0.5 * ((Bxr * Bxr + Byr * Byr) + Bzr * Bzr)) + 0.5 * (Qfl[8] * Qfl[8]);
         Qfr[5] = Bxr;
         Qfr[6] = Byr;
         Qfr[7] = Bzr;
         Qfr[8] = 0.0;
     } else if (kind == BC_WALL) { /* :196-227 */
-        double rhow = Qfl[0];
-        double uw = Qfl[1] / rhow, vw = Qfl[2] / rhow, ww = Qfl[3] / rhow;
+        real rhow = Qfl[0];
+        real uw = Qfl[1] / rhow, vw = Qfl[2] / rhow, ww = Qfl[3] / rhow;
         Qfr[0] = rhow;
         Qfr[4] = Qfl[4];
         Qfr[5] = -Qfl[5];
@@ -797,8 +828,8 @@ static void bc_ghost(const orc_ctx *cx, int kind, const double *Qfl,
         Qfr[7] = -Qfl[7];
         Qfr[8] = Qfl[8];
         if (p->vismode == 0) {
-            double magnorm = sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
-            double VN = uw * normf[0] / magnorm + vw * normf[1] / magnorm;
+            real magnorm = r_sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
+            real VN = uw * normf[0] / magnorm + vw * normf[1] / magnorm;
             Qfr[1] = rhow * (uw - 2.0 * VN * normf[0] / magnorm);
             Qfr[2] = rhow * (vw - 2.0 * VN * normf[1] / magnorm);
             Qfr[3] = -rhow * ww;
@@ -808,19 +839,19 @@ static void bc_ghost(const orc_ctx *cx, int kind, const double *Qfl,
             Qfr[3] = -rhow * ww;
         }
     } else if (kind == BC_SYMP) { /* :272-299 */
-        double rhow = Qfl[0];
-        double uw = Qfl[1] / rhow, vw = Qfl[2] / rhow, ww = Qfl[3] / rhow;
-        Qfr[0] = p->rinf * 2.0 - Qfl[0];
-        double magnorm = sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
-        double VN = uw * normf[0] / magnorm + vw * normf[1] / magnorm;
+        real rhow = Qfl[0];
+        real uw = Qfl[1] / rhow, vw = Qfl[2] / rhow, ww = Qfl[3] / rhow;
+        Qfr[0] = cx->fs[0] * 2.0 - Qfl[0];
+        real magnorm = r_sqrt(normf[0] * normf[0] + normf[1] * normf[1]);
+        real VN = uw * normf[0] / magnorm + vw * normf[1] / magnorm;
         Qfr[1] = Qfr[0] * (uw - 2.0 * VN * normf[0] / magnorm);
         Qfr[2] = Qfr[0] * (vw - 2.0 * VN * normf[1] / magnorm);
         Qfr[3] = -Qfr[0] * ww;
-        Qfr[5] = p->bxinf;
-        Qfr[6] = p->byinf;
+        Qfr[5] = cx->fs[4];
+        Qfr[6] = cx->fs[5];
         Qfr[7] = -Qfl[7];
         Qfr[8] = Qfl[8];
-        Qfr[4] = (p->pinf / (GAM - 1.0) + 0.5 / Qfr[0] * ((Qfr[1] * Qfr[1] + Qfr[2] * Qfr[2]) + Qfr[3] * Qfr[3]))
+        Qfr[4] = (cx->fs[1] / (GAM - 1.0) + 0.5 / Qfr[0] * ((Qfr[1] * Qfr[1] + Qfr[2] * Qfr[2]) + Qfr[3] * Qfr[3]))
                  + 0.5 * (((Qfr[5] * Qfr[5] + Qfr[6] * Qfr[6]) + Qfr[7] * Qfr[7]) + Qfr[8] * Qfr[8]);
     } else { /* FREE, :355 */
         for (int k = 0; k < NV; k++) Qfr[k] = Qfl[k];
@@ -832,14 +863,14 @@ static void bcflux(orc_ctx *cx)
     const int *lists[5] = {cx->ibfinl, cx->ibfout, cx->ibfwal, cx->ibfsymp, cx->ibfree};
     const int counts[5] = {cx->ninlet, cx->noutlet, cx->nwall, cx->nsymp, cx->nfree};
     int N = cx->N;
-    double em = cx->eigvmax, um = cx->umax;
+    real em = cx->eigvmax, um = cx->umax;
     for (int kind = 0; kind < 5; kind++) {
         for (int f = 1; f <= counts[kind]; f++) {
             int iface = lists[kind][f - 1];
             int icleft = IF2C_(iface, 1), ifacelc = IF2C_(iface, 3);
             int faml = (ifacelc % 2) + 1;
             for (int nfp = 1; nfp <= N; nfp++) {
-                double Qfl[NV], Qfr[NV], Fnl[NV], Fnr[NV], normf[2], avg[NV], eigv;
+                real Qfl[NV], Qfr[NV], Fnl[NV], Fnr[NV], normf[2], avg[NV], eigv;
                 int ifpl, jfpl;
                 face_trace(cx, icleft, ifacelc, nfp, Qfl, &ifpl, &jfpl);
                 int sign_l = 1;
@@ -860,6 +891,40 @@ static void bcflux(orc_ctx *cx)
     cx->umax = um;
 }
 
+/* Drag and lift are not in the reference.  Force on the wall faces: the x
+   and y momentum components of each wall face point's Rusanov flux out of
+   the fluid cell (the BCFLUX wall state, bcflux.f90:165-240, and
+   getrusanovflux), weighted by the quadrature weight of the face point's
+   position along the face. */
+void orc_wall_force(orc_ctx *cx, const double *w, real *fx, real *fy)
+{
+    int N = cx->N;
+    real sx = 0.0, sy = 0.0, em = 0.0, um = 0.0; /* maxima discarded */
+    for (int f = 1; f <= cx->nwall; f++) {
+        int iface = cx->ibfwal[f - 1];
+        int ic = IF2C_(iface, 1), lf = IF2C_(iface, 3);
+        int fam = (lf % 2) + 1;
+        for (int nfp = 1; nfp <= N; nfp++) {
+            real Qfl[NV], Qfr[NV], Fnl[NV], Fnr[NV], normf[2], eigv;
+            int ifp, jfp;
+            face_trace(cx, ic, lf, nfp, Qfl, &ifp, &jfp);
+            int sign_l = 1;
+            if (fam == 1) { if (ifp == 1) sign_l = -1; }
+            else { if (jfp == 1) sign_l = -1; }
+            face_normal(cx, ic, lf, ifp, jfp, normf);
+            bc_ghost(cx, BC_WALL, Qfl, normf, Qfr);
+            rusanov(Qfl, Qfr, Fnl, Fnr, normf, sign_l, 1, cx->c_h, &eigv, &em, &um);
+            /* Fnl is the flux along +xi (+eta); sign_l turns it into the
+               flux out of the fluid cell, the force on the body */
+            double wt = w[(fam == 1 ? jfp : ifp) - 1] * (double)sign_l;
+            sx = sx + wt * Fnl[1];
+            sy = sy + wt * Fnl[2];
+        }
+    }
+    *fx = sx;
+    *fy = sy;
+}
+
 /* nablaQsp(1,9), compflux.f90:107-157 */
 static void nablaQsp(orc_ctx *cx)
 {
@@ -868,28 +933,28 @@ static void nablaQsp(orc_ctx *cx)
     for (int ic = 1; ic <= NC; ic++)
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
-                double a[NV], b[NV];
+                real a[NV], b[NV];
                 for (int d = 1; d <= 2; d++) {
                     for (int k = 0; k < NV; k++) a[k] = 0.0;
                     for (int rfp = 1; rfp <= N1; rfp++) {
-                        double s = S1_(1, d, rfp, js, ic), m = M_(rfp, is);
+                        real s = S1_(1, d, rfp, js, ic), m = M_(rfp, is);
                         for (int k = 1; k <= NV; k++)
                             a[k - 1] = a[k - 1] + FI_(Qvfi, k, rfp, js, ic) * m * s;
                     }
                     for (int k = 0; k < NV; k++) b[k] = 0.0;
                     for (int rfp = 1; rfp <= N1; rfp++) {
-                        double s = S2_(2, d, is, rfp, ic), m = M_(rfp, js);
+                        real s = S2_(2, d, is, rfp, ic), m = M_(rfp, js);
                         for (int k = 1; k <= NV; k++)
                             b[k - 1] = b[k - 1] + FJ_(Qvfj, k, is, rfp, ic) * m * s;
                     }
-                    double J = JAC_(is, js, ic);
+                    real J = JAC_(is, js, ic);
                     for (int k = 1; k <= NV; k++) NQS_(k, d, is, js, ic) = (a[k - 1] + b[k - 1]) / J;
                 }
             }
 }
 
 /* internal energy at a Qvf point, compflux.f90:272-277 */
-static double enei_of(const double *q)
+static real enei_of(const real *q)
 {
     return (((q[4] / q[0] - 0.5 * sq(q[1] / q[0])) - 0.5 * sq(q[2] / q[0])) - 0.5 * sq(q[3] / q[0]))
            - 0.5 * (((q[5] * q[5] + q[6] * q[6]) + q[7] * q[7]) + q[8] * q[8]) / q[0];
@@ -903,7 +968,7 @@ static void comp_grad_internal_energy(orc_ctx *cx)
     for (int ic = 1; ic <= NC; ic++)
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
-                double t = 0.0;
+                real t = 0.0;
                 for (int rfp = 1; rfp <= N1; rfp++)
                     t = t + enei_of(&FI_(Qvfi, 1, rfp, js, ic)) * M_(rfp, is);
                 DEDXI_(is, js, ic) = t;
@@ -920,7 +985,7 @@ static void nablaQ_interior_FP(orc_ctx *cx)
     int N = cx->N, N1 = cx->N1, NC = cx->NC;
 #pragma omp parallel for schedule(static)
     for (int ic = 1; ic <= NC; ic++) {
-        double a[NV], b[NV];
+        real a[NV], b[NV];
         for (int jfp = 1; jfp <= N; jfp++)
             for (int ifp = 2; ifp <= N; ifp++) {
                 for (int k = 0; k < NV; k++) { a[k] = 0.0; b[k] = 0.0; }
@@ -952,7 +1017,7 @@ static void nablaQ_interior_FP(orc_ctx *cx)
 
 /* gradient trace at a face point (the nablaQs analogue of face_trace) */
 static void grad_trace(const orc_ctx *cx, int ic, int lf, int nfp,
-                       double *g1, double *g2, int *ifp_o, int *jfp_o)
+                       real *g1, real *g2, int *ifp_o, int *jfp_o)
 {
     int N = cx->N, N1 = cx->N1;
     int ifp = IFP_(nfp, lf), jfp = JFP_(nfp, lf);
@@ -975,7 +1040,7 @@ static void grad_trace(const orc_ctx *cx, int ic, int lf, int nfp,
 }
 
 static void store_grad(orc_ctx *cx, int ic, int lf, int ifp, int jfp,
-                       const double *g1, const double *g2)
+                       const real *g1, const real *g2)
 {
     int N = cx->N, N1 = cx->N1;
     if ((lf % 2) + 1 == 1) {
@@ -997,7 +1062,7 @@ static void pair_visflux(orc_ctx *cx, int icleft, int icright, int ifacelc,
                          int ifacerc)
 {
     int N = cx->N;
-    double l1[NV], l2[NV], r1[NV], r2[NV], a1[NV], a2[NV];
+    real l1[NV], l2[NV], r1[NV], r2[NV], a1[NV], a2[NV];
     for (int nfp = 1; nfp <= N; nfp++) {
         int ifpl, jfpl, ifpr, jfpr;
         grad_trace(cx, icleft, ifacelc, nfp, l1, l2, &ifpl, &jfpl);
@@ -1023,12 +1088,12 @@ static void bcvisflux(orc_ctx *cx)
             int ic = IF2C_(iface, 1), lf = IF2C_(iface, 3);
             int faml = (lf % 2) + 1;
             for (int nfp = 1; nfp <= N; nfp++) {
-                double g1[NV], g2[NV], r1[NV], r2[NV], a1[NV], a2[NV];
+                real g1[NV], g2[NV], r1[NV], r2[NV], a1[NV], a2[NV];
                 int ifpl, jfpl;
                 grad_trace(cx, ic, lf, nfp, g1, g2, &ifpl, &jfpl);
                 for (int k = 0; k < NV; k++) { r1[k] = g1[k]; r2[k] = g2[k]; }
                 if (kind == BC_WALL) {
-                    double Qfo[NV], dxi = 0.0, deta = 0.0;
+                    real Qfo[NV], dxi = 0.0, deta = 0.0;
                     for (int k = 0; k < NV; k++) Qfo[k] = 0.0;
                     /* the reference accumulates the gradient trace, the
                        state trace and the energy gradients in one sp loop;
@@ -1049,10 +1114,10 @@ static void bcvisflux(orc_ctx *cx)
                             deta = deta + DEDETA_(ifpl, sp, ic) * L_(jfpl, sp);
                         }
                     }
-                    double ur = Qfo[1] / Qfo[0], vr = Qfo[2] / Qfo[0], wr = Qfo[3] / Qfo[0];
-                    double inte = (Qfo[4] / Qfo[0] - 0.5 * ((ur * ur + vr * vr) + wr * wr))
+                    real ur = Qfo[1] / Qfo[0], vr = Qfo[2] / Qfo[0], wr = Qfo[3] / Qfo[0];
+                    real inte = (Qfo[4] / Qfo[0] - 0.5 * ((ur * ur + vr * vr) + wr * wr))
                                   - 0.5 * (((Qfo[5] * Qfo[5] + Qfo[6] * Qfo[6]) + Qfo[7] * Qfo[7]) + Qfo[8] * Qfo[8]) / Qfo[0];
-                    double dur, dvr, dwr, dKE, dBp;
+                    real dur, dvr, dwr, dKE, dBp;
                     /* first direction */
                     dur = (g1[1] - ur * g1[0]) / Qfo[0];
                     dvr = (g1[2] - vr * g1[0]) / Qfo[0];
@@ -1111,8 +1176,8 @@ static void comp_artificial_viscosity(orc_ctx *cx)
                 lo[1][isl][jsl] = 0.0;
                 for (int js = 1; js <= N; js++)
                     for (int is = 1; is <= N; is++) {
-                        lo[0][isl][jsl] = lo[0][isl][jsl] + Q_(1, is, js, ic) * H[isl][is] * H[jsl][js];
-                        double d = NQS_(7, 1, is, js, ic) - NQS_(6, 2, is, js, ic);
+                        lo[0][isl][jsl] = lo[0][isl][jsl] + RV(Q_(1, is, js, ic)) * H[isl][is] * H[jsl][js];
+                        double d = RV(NQS_(7, 1, is, js, ic)) - RV(NQS_(6, 2, is, js, ic));
                         lo[1][isl][jsl] = lo[1][isl][jsl] + d * d * H[isl][is] * H[jsl][js];
                     }
             }
@@ -1128,11 +1193,11 @@ static void comp_artificial_viscosity(orc_ctx *cx)
         double Se[2] = {0.0, 0.0};
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
-                double q1 = Q_(1, is, js, ic);
-                Se[0] = Se[0] + sq(hi[0][is][js] - q1) / (q1 * q1);
-                double d = NQS_(7, 1, is, js, ic) - NQS_(6, 2, is, js, ic);
+                double q1 = RV(Q_(1, is, js, ic));
+                Se[0] = Se[0] + (hi[0][is][js] - q1) * (hi[0][is][js] - q1) / (q1 * q1);
+                double d = RV(NQS_(7, 1, is, js, ic)) - RV(NQS_(6, 2, is, js, ic));
                 double Jz = d * d;
-                Se[1] = Se[1] + sq(hi[1][is][js] - Jz) / (Jz * Jz);
+                Se[1] = Se[1] + (hi[1][is][js] - Jz) * (hi[1][is][js] - Jz) / (Jz * Jz);
             }
         SMIND_(1, ic) = log10(Se[0]);
         SMIND_(2, ic) = log10(Se[1]);
@@ -1145,7 +1210,7 @@ static void comp_artificial_viscosity(orc_ctx *cx)
         s0[v] = (se_high[v] + se_low[v]) * 0.5;
     }
     double h_msh = sqrt(cx->p.dxcycl * cx->p.dycycl / (double)cx->p.ncellglob);
-    cx->epsilon0 = cx->eigvmax_g * h_msh / (double)(N - 1) * 0.05;
+    cx->epsilon0 = RV(cx->eigvmax_g) * h_msh / (double)(N - 1) * 0.05;
     double e0 = cx->epsilon0;
     for (int ic = 1; ic <= NC; ic++)
         for (int v = 1; v <= 2; v++) {
@@ -1203,11 +1268,11 @@ static void comp_av_flux(orc_ctx *cx)
 static void comp_viscous_flux(orc_ctx *cx)
 {
     int N = cx->N, N1 = cx->N1, NC = cx->NC;
-    double mu = cx->p.mu, eta0 = cx->p.eta0;
+    real mu = cx->p.mu, eta0 = cx->p.eta0;
     int artiv = cx->p.artiv;
 #pragma omp parallel for schedule(static)
     for (int ic = 1; ic <= NC; ic++) {
-        double Qs[NV], nQ[2 * NV], Fv[NV], Gv[NV], Fa[NV], Ga[NV];
+        real Qs[NV], nQ[2 * NV], Fv[NV], Gv[NV], Fa[NV], Ga[NV];
         for (int jfp = 1; jfp <= N; jfp++)
             for (int ifp = 1; ifp <= N1; ifp++) {
                 for (int k = 1; k <= NV; k++) {
@@ -1216,7 +1281,7 @@ static void comp_viscous_flux(orc_ctx *cx)
                     nQ[NV + k - 1] = NQI_(k, 2, ifp, jfp, ic);
                 }
                 vflux(Qs, nQ, mu, eta0, Fv, Gv);
-                double s11 = S1_(1, 1, ifp, jfp, ic), s12 = S1_(1, 2, ifp, jfp, ic);
+                real s11 = S1_(1, 1, ifp, jfp, ic), s12 = S1_(1, 2, ifp, jfp, ic);
                 for (int k = 1; k <= NV; k++)
                     FI_(Fv1, k, ifp, jfp, ic) = Fv[k - 1] * s11 + Gv[k - 1] * s12;
                 if (artiv == 1) {
@@ -1233,7 +1298,7 @@ static void comp_viscous_flux(orc_ctx *cx)
                     nQ[NV + k - 1] = NQJ_(k, 2, ifp, jfp, ic);
                 }
                 vflux(Qs, nQ, mu, eta0, Fv, Gv);
-                double s21 = S2_(2, 1, ifp, jfp, ic), s22 = S2_(2, 2, ifp, jfp, ic);
+                real s21 = S2_(2, 1, ifp, jfp, ic), s22 = S2_(2, 2, ifp, jfp, ic);
                 for (int k = 1; k <= NV; k++)
                     FJ_(Gv2, k, ifp, jfp, ic) = Fv[k - 1] * s21 + Gv[k - 1] * s22;
                 if (artiv == 1) {
@@ -1253,7 +1318,7 @@ static int viscous_chain_skipped(const orc_ctx *cx)
 /* compflux, compflux.f90:1-33 */
 static void compflux(orc_ctx *cx)
 {
-    cx->c_h = sqrt(cx->eigvmax_g * (cx->eigvmax_g - cx->umax_g));
+    cx->c_h = r_sqrt(cx->eigvmax_g * (cx->eigvmax_g - cx->umax_g));
     inviscid_flux_interior(cx);
     interface_and_cyclic_flux(cx);
     bcflux(cx);
@@ -1290,15 +1355,15 @@ void orc_compresid(orc_ctx *cx)
     compflux(cx);
     int N = cx->N, N1 = cx->N1, NC = cx->NC;
     int vis = cx->p.vismode == 1, skip = viscous_chain_skipped(cx);
-    double alpha = cx->alpha;
+    real alpha = cx->alpha;
 #pragma omp parallel for schedule(static)
     for (int ic = 1; ic <= NC; ic++)
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
-                double dF[NV], dG[NV], dFv[NV], dGv[NV];
+                real dF[NV], dG[NV], dFv[NV], dGv[NV];
                 for (int k = 0; k < NV; k++) { dF[k] = 0.0; dFv[k] = 0.0; }
                 for (int rfp = 1; rfp <= N1; rfp++) {
-                    double m = M_(rfp, is);
+                    real m = M_(rfp, is);
                     for (int k = 1; k <= NV; k++) {
                         dF[k - 1] = dF[k - 1] + FI_(F1, k, rfp, js, ic) * m;
                         if (vis && !skip) dFv[k - 1] = dFv[k - 1] + FI_(Fv1, k, rfp, js, ic) * m;
@@ -1306,7 +1371,7 @@ void orc_compresid(orc_ctx *cx)
                 }
                 for (int k = 0; k < NV; k++) { dG[k] = 0.0; dGv[k] = 0.0; }
                 for (int rfp = 1; rfp <= N1; rfp++) {
-                    double m = M_(rfp, js);
+                    real m = M_(rfp, js);
                     for (int k = 1; k <= NV; k++) {
                         dG[k - 1] = dG[k - 1] + FJ_(G2, k, is, rfp, ic) * m;
                         if (vis && !skip) dGv[k - 1] = dGv[k - 1] + FJ_(Gv2, k, is, rfp, ic) * m;
@@ -1323,14 +1388,14 @@ void orc_compresid(orc_ctx *cx)
     for (int ic = 1; ic <= NC; ic++)
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
-                double J = JAC_(is, js, ic);
+                real J = JAC_(is, js, ic);
                 for (int k = 1; k <= NV; k++) R_(k, is, js, ic) = R_(k, is, js, ic) / J;
-                double divB = NQS_(6, 1, is, js, ic) + NQS_(7, 2, is, js, ic);
-                double Bx = Q_(6, is, js, ic), By = Q_(7, is, js, ic), Bz = Q_(8, is, js, ic);
-                double ux = Q_(2, is, js, ic) / Q_(1, is, js, ic);
-                double uy = Q_(3, is, js, ic) / Q_(1, is, js, ic);
-                double uz = Q_(4, is, js, ic) / Q_(1, is, js, ic);
-                double psi = Q_(9, is, js, ic);
+                real divB = NQS_(6, 1, is, js, ic) + NQS_(7, 2, is, js, ic);
+                real Bx = Q_(6, is, js, ic), By = Q_(7, is, js, ic), Bz = Q_(8, is, js, ic);
+                real ux = Q_(2, is, js, ic) / Q_(1, is, js, ic);
+                real uy = Q_(3, is, js, ic) / Q_(1, is, js, ic);
+                real uz = Q_(4, is, js, ic) / Q_(1, is, js, ic);
+                real psi = Q_(9, is, js, ic);
                 R_(2, is, js, ic) = R_(2, is, js, ic) - divB * Bx;
                 R_(3, is, js, ic) = R_(3, is, js, ic) - divB * By;
                 R_(4, is, js, ic) = R_(4, is, js, ic) - divB * Bz;
@@ -1354,29 +1419,29 @@ static const double A30 = 0.355909775063327, A32 = 0.644090224936674,
                     B32 = 0.242995220537396, B43 = 0.238458932846290,
                     B54 = 0.287632146308408;
 
-void orc_rk_s5p3_combine(int stage, long n, double dt, double *q,
-                         const double *qk0, const double *qka,
-                         const double *r)
+void orc_rk_s5p3_combine(int stage, long n, real dt, real *q,
+                         const real *qk0, const real *qka,
+                         const real *r)
 {
     long i;
     switch (stage) {
-    case 1: { double c = B10 * dt;
+    case 1: { real c = B10 * dt;
 #pragma omp parallel for schedule(static)
         for (i = 0; i < n; i++) q[i] = q[i] + c * r[i];
         break; }
-    case 2: { double c = B21 * dt;
+    case 2: { real c = B21 * dt;
 #pragma omp parallel for schedule(static)
         for (i = 0; i < n; i++) q[i] = q[i] + c * r[i];
         break; }
-    case 3: { double c = B32 * dt;
+    case 3: { real c = B32 * dt;
 #pragma omp parallel for schedule(static)
         for (i = 0; i < n; i++) q[i] = (A30 * qk0[i] + A32 * q[i]) + c * r[i];
         break; }
-    case 4: { double c = B43 * dt;
+    case 4: { real c = B43 * dt;
 #pragma omp parallel for schedule(static)
         for (i = 0; i < n; i++) q[i] = (A40 * qk0[i] + A43 * q[i]) + c * r[i];
         break; }
-    default: { double c = B54 * dt;
+    default: { real c = B54 * dt;
 #pragma omp parallel for schedule(static)
         for (i = 0; i < n; i++) q[i] = (A52 * qka[i] + A54 * q[i]) + c * r[i];
         break; }
@@ -1387,10 +1452,10 @@ void orc_rk_s5p3_combine(int stage, long n, double dt, double *q,
 void orc_rk_s5p3(orc_ctx *cx, double dt, int nsteps)
 {
     long n = (long)NV * cx->N * cx->N * cx->NC;
-    double *Qk0 = (double *)malloc(sizeof(double) * n);
-    double *Qka = (double *)malloc(sizeof(double) * n);
+    real *Qk0 = (real *)malloc(sizeof(real) * n);
+    real *Qka = (real *)malloc(sizeof(real) * n);
     for (int s = 0; s < nsteps; s++) {
-        memcpy(Qk0, cx->Q, sizeof(double) * n);
+        memcpy(Qk0, cx->Q, sizeof(real) * n);
         double ctime0 = cx->ctime;
         orc_compresid(cx);
         orc_rk_s5p3_combine(1, n, dt, cx->Q, Qk0, Qka, cx->resid);
@@ -1400,7 +1465,7 @@ void orc_rk_s5p3(orc_ctx *cx, double dt, int nsteps)
         orc_rk_s5p3_combine(2, n, dt, cx->Q, Qk0, Qka, cx->resid);
         double dt2 = dt1 + B21 * dt;
         cx->ctime = ctime0 + dt2;
-        memcpy(Qka, cx->Q, sizeof(double) * n);
+        memcpy(Qka, cx->Q, sizeof(real) * n);
         orc_compresid(cx);
         orc_rk_s5p3_combine(3, n, dt, cx->Q, Qk0, Qka, cx->resid);
         double dt3 = A32 * dt2 + B32 * dt;
@@ -1422,14 +1487,14 @@ void orc_rk_s5p3(orc_ctx *cx, double dt, int nsteps)
 void orc_five_stage_rk(orc_ctx *cx, double dt, int nsteps)
 {
     long n = (long)NV * cx->N * cx->N * cx->NC;
-    double *qj0 = (double *)malloc(sizeof(double) * n);
-    double *qj2 = (double *)malloc(sizeof(double) * n);
-    double *qj3 = (double *)malloc(sizeof(double) * n);
-    double *r0 = (double *)malloc(sizeof(double) * n);
-    double *Q = cx->Q, *R = cx->resid;
+    real *qj0 = (real *)malloc(sizeof(real) * n);
+    real *qj2 = (real *)malloc(sizeof(real) * n);
+    real *qj3 = (real *)malloc(sizeof(real) * n);
+    real *r0 = (real *)malloc(sizeof(real) * n);
+    real *Q = cx->Q, *R = cx->resid;
     for (int s = 0; s < nsteps; s++) {
         double old_time = cx->ctime;
-        memcpy(qj0, Q, sizeof(double) * n);
+        memcpy(qj0, Q, sizeof(real) * n);
         orc_compresid(cx);
         double a11 = 0.39175222700392;
         double rdt = dt * a11;
@@ -1438,21 +1503,21 @@ void orc_five_stage_rk(orc_ctx *cx, double dt, int nsteps)
         orc_compresid(cx);
         double a21 = 0.44437049406734, a22 = 0.55562950593266, a23 = 0.36841059262959;
         for (long i = 0; i < n; i++) Q[i] = (a21 * qj0[i] + a22 * Q[i]) + a23 * R[i] * dt;
-        memcpy(qj2, Q, sizeof(double) * n);
+        memcpy(qj2, Q, sizeof(real) * n);
         rdt = rdt * a22 + a23 * dt;
         cx->ctime = old_time + rdt;
         orc_compresid(cx);
         double a31 = 0.6201018513854, a32 = 0.3798981486146, a33 = 0.25189177424738;
         double c3 = a33 * dt;
         for (long i = 0; i < n; i++) Q[i] = (a31 * qj0[i] + a32 * Q[i]) + c3 * R[i];
-        memcpy(qj3, Q, sizeof(double) * n);
+        memcpy(qj3, Q, sizeof(real) * n);
         rdt = rdt * a32 + a33 * dt;
         cx->ctime = old_time + rdt;
         orc_compresid(cx);
         double a41 = 0.17807995410773, a42 = 0.82192004589227, a43 = 0.54497475021237;
         double c4 = a43 * dt;
         for (long i = 0; i < n; i++) Q[i] = (a41 * qj0[i] + a42 * Q[i]) + c4 * R[i];
-        memcpy(r0, R, sizeof(double) * n);
+        memcpy(r0, R, sizeof(real) * n);
         rdt = rdt * a42 + a43 * dt;
         cx->ctime = old_time + rdt;
         orc_compresid(cx);
@@ -1470,13 +1535,13 @@ void orc_five_stage_rk(orc_ctx *cx, double dt, int nsteps)
 void orc_monitor(const orc_ctx *cx, double *residsum, double *divbsum)
 {
     int N = cx->N, NC = cx->NC;
-    double rn = 0.0, db = 0.0;
+    real rn = 0.0, db = 0.0;
     for (int ic = 1; ic <= NC; ic++)
         for (int js = 1; js <= N; js++)
             for (int is = 1; is <= N; is++) {
                 for (int k = 1; k <= NV; k++) rn = rn + sq(R_(k, is, js, ic));
                 db = db + sq(NQS_(6, 1, is, js, ic) + NQS_(7, 2, is, js, ic));
             }
-    *residsum = rn;
-    *divbsum = db;
+    *residsum = RV(rn);
+    *divbsum = RV(db);
 }

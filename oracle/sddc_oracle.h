@@ -25,6 +25,16 @@ extern "C" {
 
 typedef struct orc_ctx orc_ctx;
 
+/* State arithmetic: double, or double _Complex in the complex-step tangent
+   build (libsddc_oracle_cs.so, -DORC_CSTEP), whose state arrays are
+   interleaved (re, im) pairs. */
+#ifdef ORC_CSTEP
+#include <complex.h>
+typedef double _Complex orc_real;
+#else
+typedef double orc_real;
+#endif
+
 typedef struct orc_params {
     int N;            /* solution points per direction (p+1)          */
     int ncell;        /* NCELL                                        */
@@ -62,15 +72,18 @@ int orc_set_tables(orc_ctx *c, const double *Lmat, const double *Mmat,
                    const int *ibfsymp, int nsymp,
                    const int *ibfree, int nfree,
                    const int *cyc2fpair, int npair);
-void orc_set_state(orc_ctx *c, const double *Q, double ctime,
+void orc_set_state(orc_ctx *c, const orc_real *Q, double ctime,
                    double eigvmax, double umax);
-void orc_get_state(const orc_ctx *c, double *Q, double *resid,
-                   double *nablaQs, double *muAV, double *sm_ind);
+void orc_get_state(const orc_ctx *c, orc_real *Q, orc_real *resid,
+                   orc_real *nablaQs, double *muAV, double *sm_ind);
+/* boundary free stream (rinf, pinf, uinf, vinf, bxinf, byinf); starts as
+   the parameters given to orc_create */
+void orc_set_freestream(orc_ctx *c, const orc_real *fs);
 void orc_get_maxima(const orc_ctx *c, double *eigvmax, double *umax,
                     double *c_h, double *epsilon0, double *ctime);
 /* Flux arrays after the last residual (F1, G2 inviscid; Fv1, Gv2 viscous) */
-void orc_get_fluxes(const orc_ctx *c, double *F1, double *G2,
-                    double *Fv1, double *Gv2);
+void orc_get_fluxes(const orc_ctx *c, orc_real *F1, orc_real *G2,
+                    orc_real *Fv1, orc_real *Gv2);
 
 /* --- the hot path ----------------------------------------------------- */
 void orc_compresid(orc_ctx *c);                    /* compresid.f90:1-80 */
@@ -80,16 +93,23 @@ void orc_five_stage_rk(orc_ctx *c, double dt, int nsteps); /* :88-156 */
 void orc_monitor(const orc_ctx *c, double *residsum, double *divbsum);
 
 /* --- point kernels, exposed for consistency tests --------------------- */
-void orc_point_iflux(const double *Qi, double c_h, double *umax,
-                     double *F, double *G);
-void orc_point_rusanov(const double *Qfl, const double *Qfr, double *Fnl,
-                       double *Fnr, const double *normf, int sign_l,
-                       int sign_r, double c_h, double *eigv,
-                       double *eigvmax, double *umax);
+void orc_point_iflux(const orc_real *Qi, orc_real c_h, orc_real *umax,
+                     orc_real *F, orc_real *G);
+void orc_point_rusanov(const orc_real *Qfl, const orc_real *Qfr, orc_real *Fnl,
+                       orc_real *Fnr, const orc_real *normf, int sign_l,
+                       int sign_r, orc_real c_h, orc_real *eigv,
+                       orc_real *eigvmax, orc_real *umax);
 /* RK_S5P3 stage combination on plain arrays (for the order test) */
-void orc_rk_s5p3_combine(int stage, long n, double dt, double *q,
-                         const double *qk0, const double *qka,
-                         const double *r);
+void orc_rk_s5p3_combine(int stage, long n, orc_real dt, orc_real *q,
+                         const orc_real *qk0, const orc_real *qka,
+                         const orc_real *r);
+
+/* --- drag and lift: not in the reference ------------------------------ */
+/* Force on the wall faces (IBFWAL): the x and y momentum components of
+   each wall face point's Rusanov flux out of the fluid cell at the current
+   state, weighted by w[line] (quadrature weights of the solution points on
+   [0,1]) and summed.  The maxima are not updated. */
+void orc_wall_force(orc_ctx *c, const double *w, orc_real *fx, orc_real *fy);
 
 #ifdef __cplusplus
 }

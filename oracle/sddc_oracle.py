@@ -5,6 +5,11 @@ baseline / reference legs of bench.py; never by the product package.
 Parity of this oracle against the reference itself is unpinned (the
 reference has no golden vectors and no Fortran compiler exists here); it is
 pinned by the known-answer tests in tests/test_oracle_kat.py.
+
+``Oracle(..., tangent=True)`` loads the complex-step build of the same source
+(libsddc_oracle_cs.so): its state arrays are complex128, and a state
+Q + 1j*h*V evaluated with h ~ 1e-30 carries the FP64 tangent dR/dQ . V in
+its imaginary part divided by h.
 """
 from __future__ import annotations
 
@@ -16,6 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libsddc_oracle.so")
+LIB_CS = os.path.join(HERE, "libsddc_oracle_cs.so")
 
 _I = ctypes.c_int
 _L = ctypes.c_long
@@ -30,7 +36,7 @@ class Params(ctypes.Structure):
                 ("rinf", _D), ("pinf", _D), ("uinf", _D), ("vinf", _D), ("bxinf", _D), ("byinf", _D)]
 
 
-_lib = None
+_libs = {}
 
 
 def build() -> str:
@@ -38,33 +44,39 @@ def build() -> str:
     return LIB
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
-            build()
-        L = ctypes.CDLL(LIB)
-        L.orc_create.restype = ctypes.c_void_p
-        L.orc_create.argtypes = [ctypes.POINTER(Params)]
-        L.orc_destroy.argtypes = [ctypes.c_void_p]
-        L.orc_set_threads.argtypes = [_I]
-        L.orc_set_tables.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD, _PI, _I] + [_PI, _I] * 7
-        L.orc_set_state.argtypes = [ctypes.c_void_p, _PD, _D, _D, _D]
-        L.orc_get_state.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD]
-        L.orc_get_maxima.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD]
-        L.orc_get_fluxes.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD]
-        L.orc_compresid.argtypes = [ctypes.c_void_p]
-        L.orc_rk_s5p3.argtypes = [ctypes.c_void_p, _D, _I]
-        L.orc_five_stage_rk.argtypes = [ctypes.c_void_p, _D, _I]
-        L.orc_monitor.argtypes = [ctypes.c_void_p, _PD, _PD]
-        L.orc_setsandpoints.argtypes = [_I, _PD, _PD]
-        L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
-        L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
+def _load(path, tangent):
+    if not os.path.exists(path):
+        build()
+    L = ctypes.CDLL(path)
+    L.orc_create.restype = ctypes.c_void_p
+    L.orc_create.argtypes = [ctypes.POINTER(Params)]
+    L.orc_destroy.argtypes = [ctypes.c_void_p]
+    L.orc_set_threads.argtypes = [_I]
+    L.orc_set_tables.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD, _PI, _I] + [_PI, _I] * 7
+    L.orc_set_state.argtypes = [ctypes.c_void_p, _PD, _D, _D, _D]
+    L.orc_get_state.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD]
+    L.orc_set_freestream.argtypes = [ctypes.c_void_p, _PD]
+    L.orc_get_maxima.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD, _PD]
+    L.orc_get_fluxes.argtypes = [ctypes.c_void_p, _PD, _PD, _PD, _PD]
+    L.orc_compresid.argtypes = [ctypes.c_void_p]
+    L.orc_rk_s5p3.argtypes = [ctypes.c_void_p, _D, _I]
+    L.orc_five_stage_rk.argtypes = [ctypes.c_void_p, _D, _I]
+    L.orc_monitor.argtypes = [ctypes.c_void_p, _PD, _PD]
+    L.orc_wall_force.argtypes = [ctypes.c_void_p, _PD, _PD, _PD]
+    L.orc_setsandpoints.argtypes = [_I, _PD, _PD]
+    L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
+    L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
+    if not tangent:  # complex scalars by value have no ctypes type
         L.orc_point_iflux.argtypes = [_PD, _D, _PD, _PD, _PD]
         L.orc_point_rusanov.argtypes = [_PD, _PD, _PD, _PD, _PD, _I, _I, _D, _PD, _PD, _PD]
         L.orc_rk_s5p3_combine.argtypes = [_I, _L, _D, _PD, _PD, _PD, _PD]
-        _lib = L
-    return _lib
+    return L
+
+
+def lib(tangent: bool = False):
+    if tangent not in _libs:
+        _libs[tangent] = _load(LIB_CS if tangent else LIB, tangent)
+    return _libs[tangent]
 
 
 def _p(a, t=_PD):
@@ -72,7 +84,9 @@ def _p(a, t=_PD):
 
 
 def set_threads(n: int) -> None:
-    lib().orc_set_threads(int(n))
+    lib()
+    for L in _libs.values():
+        L.orc_set_threads(int(n))
 
 
 def operators(N: int):
@@ -97,17 +111,22 @@ def metrics(N: int, ivcell: np.ndarray, xv: np.ndarray, yv: np.ndarray):
 
 
 class Oracle:
-    """The reference's single-rank residual path on the CPU, FP64."""
+    """The reference's single-rank residual path on the CPU, FP64 (or its
+    complex-step tangent with ``tangent=True``)."""
 
-    def __init__(self, tables, physics, skip_ideal_viscous: bool = False, ncellglob: int | None = None):
+    def __init__(self, tables, physics, skip_ideal_viscous: bool = False, ncellglob: int | None = None,
+                 tangent: bool = False):
         self.N = tables.N
         self.ncell = tables.ncell
+        self.tangent = tangent
+        self._L = lib(tangent)
+        self.dtype = np.complex128 if tangent else np.float64
         p = Params(N=tables.N, ncell=tables.ncell, ncellglob=ncellglob or tables.ncell, vismode=physics.vismode,
                    artiv=physics.artiv, skip_ideal_viscous=int(skip_ideal_viscous), mu=physics.mu,
                    eta0=physics.eta0, dxcycl=physics.dxcycl, dycycl=physics.dycycl, rinf=physics.rinf,
                    pinf=physics.pinf, uinf=physics.uinf, vinf=physics.vinf, bxinf=physics.bxinf,
                    byinf=physics.byinf)
-        self._h = lib().orc_create(ctypes.byref(p))
+        self._h = self._L.orc_create(ctypes.byref(p))
         if not self._h:
             raise ValueError("orc_create rejected the parameters")
         t = tables
@@ -121,56 +140,84 @@ class Oracle:
             args += [_p(a, _PI), n]
         if2c = np.asfortranarray(t.IF2C, dtype=np.int32)
         self._keep.append(if2c)
-        lib().orc_set_tables(self._h, _p(np.asfortranarray(t.Lmat)), _p(np.asfortranarray(t.Mmat)),
-                             _p(np.asfortranarray(t.S1)), _p(np.asfortranarray(t.S2)),
-                             _p(np.asfortranarray(t.Jac)), _p(if2c, _PI), t.nface, *args)
+        self._L.orc_set_tables(self._h, _p(np.asfortranarray(t.Lmat)), _p(np.asfortranarray(t.Mmat)),
+                               _p(np.asfortranarray(t.S1)), _p(np.asfortranarray(t.S2)),
+                               _p(np.asfortranarray(t.Jac)), _p(if2c, _PI), t.nface, *args)
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().orc_destroy(h)
+            self._L.orc_destroy(h)
             self._h = None
 
+    def _arr(self, shape):
+        return np.zeros(shape, dtype=self.dtype, order="F")
+
     def set_state(self, Q, ctime=0.0, eigvmax=0.0, umax=0.0):
-        Q = np.asfortranarray(Q, dtype=np.float64)
-        lib().orc_set_state(self._h, _p(Q), ctime, eigvmax, umax)
+        Q = np.asfortranarray(Q, dtype=self.dtype)
+        self._L.orc_set_state(self._h, _p(Q), ctime, eigvmax, umax)
+
+    def set_freestream(self, fs):
+        """Boundary free stream (rinf, pinf, uinf, vinf, bxinf, byinf)."""
+        fs = np.ascontiguousarray(fs, dtype=self.dtype)
+        assert fs.shape == (6,)
+        self._L.orc_set_freestream(self._h, _p(fs))
 
     def compresid(self):
-        lib().orc_compresid(self._h)
+        self._L.orc_compresid(self._h)
 
     def rk_s5p3(self, dt, nsteps=1):
-        lib().orc_rk_s5p3(self._h, dt, nsteps)
+        self._L.orc_rk_s5p3(self._h, dt, nsteps)
 
     def five_stage_rk(self, dt, nsteps=1):
-        lib().orc_five_stage_rk(self._h, dt, nsteps)
+        self._L.orc_five_stage_rk(self._h, dt, nsteps)
 
     def state(self):
         N, nc = self.N, self.ncell
-        Q = np.zeros((9, N, N, nc), order="F")
-        R = np.zeros((9, N, N, nc), order="F")
-        G = np.zeros((9, 2, N, N, nc), order="F")
+        Q = self._arr((9, N, N, nc))
+        R = self._arr((9, N, N, nc))
+        G = self._arr((9, 2, N, N, nc))
         mu = np.zeros((2, nc), order="F")
         sm = np.zeros((2, nc), order="F")
-        lib().orc_get_state(self._h, _p(Q), _p(R), _p(G), _p(mu), _p(sm))
+        self._L.orc_get_state(self._h, _p(Q), _p(R), _p(G), _p(mu), _p(sm))
         return dict(Q=Q, resid=R, nablaQs=G, muAV=mu, sm_ind=sm)
 
     def fluxes(self):
         N, nc = self.N, self.ncell
-        out = [np.zeros((9, N + 1, N, nc), order="F"), np.zeros((9, N, N + 1, nc), order="F"),
-               np.zeros((9, N + 1, N, nc), order="F"), np.zeros((9, N, N + 1, nc), order="F")]
-        lib().orc_get_fluxes(self._h, *[_p(a) for a in out])
+        out = [self._arr((9, N + 1, N, nc)), self._arr((9, N, N + 1, nc)),
+               self._arr((9, N + 1, N, nc)), self._arr((9, N, N + 1, nc))]
+        self._L.orc_get_fluxes(self._h, *[_p(a) for a in out])
         return dict(F1=out[0], G2=out[1], Fv1=out[2], Gv2=out[3])
 
     def maxima(self):
         v = [_D() for _ in range(5)]
-        lib().orc_get_maxima(self._h, *[ctypes.byref(x) for x in v])
+        self._L.orc_get_maxima(self._h, *[ctypes.byref(x) for x in v])
         return dict(eigvmax=v[0].value, umax=v[1].value, c_h=v[2].value, epsilon0=v[3].value,
                     ctime=v[4].value)
 
     def monitor(self):
         a, b = _D(), _D()
-        lib().orc_monitor(self._h, ctypes.byref(a), ctypes.byref(b))
+        self._L.orc_monitor(self._h, ctypes.byref(a), ctypes.byref(b))
         return a.value, b.value
+
+    def wall_force(self, w):
+        """(Fx, Fy) on the wall faces at the current state; w = quadrature
+        weights of the N solution points on [0, 1]."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        assert w.shape == (self.N,)
+        fx, fy = np.zeros(1, dtype=self.dtype), np.zeros(1, dtype=self.dtype)
+        self._L.orc_wall_force(self._h, _p(w), _p(fx), _p(fy))
+        return fx[0], fy[0]
+
+
+def sp_weights(Xs):
+    """Quadrature weights of the solution points on [0, 1] (integrals of the
+    Lagrange basis): the moment equations sum_i w_i Xs_i^k = 1/(k+1)."""
+    Xs = np.asarray(Xs, dtype=np.float64)
+    N = Xs.size
+    A = np.vander(Xs, N, increasing=True).T
+    b = 1.0 / np.arange(1, N + 1)
+    return np.linalg.solve(A, b)
 
 
 def point_iflux(q, c_h=0.0):

@@ -33,6 +33,7 @@ CUDA_UNITS = {
     "stage_mixed.cu": [],
     "context.cu": [],
     "noalloc.cu": [],
+    "adjoint.cu": ["-fmad=false"],
 }
 
 

@@ -15,39 +15,12 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sddc.h"
+#include "context_impl.h"
 #include "sd_basis.h"
-#include "stage_kernel.cuh"
-
-namespace sddc {
-cudaError_t launch_stage_exact(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
-cudaError_t launch_stage_fp64(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
-cudaError_t launch_stage_mixed(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
-cudaError_t launch_trace_exact(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
-cudaError_t launch_trace_fp64(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
-cudaError_t launch_trace_mixed(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
-}  // namespace sddc
 
 using namespace sddc;
 
 namespace {
-
-constexpr int kSlots = 5;     // rotating running-max slots
-constexpr int kRegs = 6;      // RK registers (FiveStageRk needs six)
-constexpr int kMonThreads = 256;
-
-// RK_S5P3 coefficients, iterations.f90:164-174
-constexpr double A30 = 0.355909775063327, A32 = 0.644090224936674, A40 = 0.367933791638137,
-                 A43 = 0.632066208361863, A52 = 0.237593836598569, A54 = 0.762406163401431,
-                 B10 = 0.377268915331368, B21 = 0.377268915331368, B32 = 0.242995220537396,
-                 B43 = 0.238458932846290, B54 = 0.287632146308408;
-// FiveStageRk coefficients, iterations.f90:108-150
-constexpr double F11 = 0.39175222700392, F21 = 0.44437049406734, F22 = 0.55562950593266,
-                 F23 = 0.36841059262959, F31 = 0.6201018513854, F32 = 0.3798981486146,
-                 F33 = 0.25189177424738, F41 = 0.17807995410773, F42 = 0.82192004589227,
-                 F43 = 0.54497475021237, F51 = 0.00683325884039, F52 = 0.51723167208978,
-                 F53 = 0.12759831133288, F54 = 0.34833675773694, F55 = 0.08460416338212,
-                 F56 = 0.22600748319395;
 
 // muAV from the sensor and epsilon0 (AV.f90:106-140); epsilon0 uses the
 // running max of the wave speed after the evaluation.
@@ -125,17 +98,6 @@ __global__ void integrals_kernel(int ncell, int N, const double *q, const double
     }
 }
 
-int met_size(int N)
-{
-    switch (N) {
-    case 2: return MetLayout<2>::kSize;
-    case 3: return MetLayout<3>::kSize;
-    case 4: return MetLayout<4>::kSize;
-    case 5: return MetLayout<5>::kSize;
-    default: return MetLayout<6>::kSize;
-    }
-}
-
 // quadrature weights of the solution points: w_i = integral over [0,1] of
 // the Lagrange basis i (moment equations sum_i w_i x_i^k = 1/(k+1))
 std::vector<double> sp_weights(const double *Xs, int N)
@@ -168,54 +130,27 @@ std::vector<double> sp_weights(const double *Xs, int N)
 
 }  // namespace
 
-struct sddc_ctx {
-    sddc_params p{};
-    int N = 0, ncell = 0, cpb = 8, msize = 0, grid = 0;
-    size_t nq = 0;  // doubles per state
-    cudaStream_t stream = nullptr;
-    std::string err;
-    double *reg[kRegs] = {};
-    void *trace[kRegs] = {};  // face traces of each register (float in the mixed form)
-    size_t trace_bytes = 0;
-    double *met = nullptr;
-    int2 *faces = nullptr;
-    double *maxima = nullptr;  // [kSlots][2]
-    double *sm_ind = nullptr, *muav = nullptr, *resid = nullptr, *grad = nullptr;
-    double *mon_part = nullptr, *mon_out = nullptr, *int_part = nullptr, *wq = nullptr;
-    unsigned *err_flags = nullptr;
-    double *host_small = nullptr;  // pinned scratch for small read-backs
-    Ops ops{};
-    int slot = 0;  // slot holding the running maxima after the last evaluation
-    int mon_nblk = 0;  // CTAs of the last launch that wrote monitor partials
-    bool tables = false, state = false;
-    bool traces_stale = true;  // trace[0] does not match reg[0] yet
-    double ctime = 0.0;
-    cudaGraphExec_t graph[kSlots] = {};
-    double graph_dt[kSlots] = {};
-    // batch of independent cases (sddc_set_cases); ncase == 0 for one case
-    int ncase = 0;
-    std::vector<sddc_case> cases;
-    CaseParams *case_dev = nullptr;
-    int4 *tiles_rk = nullptr, *tiles_diag = nullptr;
-    int ntiles_rk = 0, ntiles_diag = 0;
-};
+int sddc::met_size(int N)
+{
+    switch (N) {
+    case 2: return MetLayout<2>::kSize;
+    case 3: return MetLayout<3>::kSize;
+    case 4: return MetLayout<4>::kSize;
+    case 5: return MetLayout<5>::kSize;
+    default: return MetLayout<6>::kSize;
+    }
+}
 
-static int set_err(sddc_ctx *c, int code, const std::string &m)
+int sddc::set_err(sddc_ctx *c, int code, const std::string &m)
 {
     if (c) c->err = m;
     return code;
 }
 
-static int cuda_err(sddc_ctx *c, cudaError_t e, const char *what)
+int sddc::cuda_err(sddc_ctx *c, cudaError_t e, const char *what)
 {
     return set_err(c, SDDC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define CK(call)                                                              \
-    do {                                                                      \
-        cudaError_t e_ = (call);                                              \
-        if (e_ != cudaSuccess) return cuda_err(ctx, e_, #call);               \
-    } while (0)
 
 extern "C" const char *sddc_last_error(const sddc_ctx *ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
 
@@ -233,6 +168,7 @@ static void free_all(sddc_ctx *ctx)
                     ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag};
     for (void *b : bufs) cudaFree(b);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
+    adjoint_free(ctx);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
 }
 
@@ -244,7 +180,7 @@ extern "C" void sddc_destroy(sddc_ctx *ctx)
     delete ctx;
 }
 
-static int alloc(sddc_ctx *ctx, void **p, size_t bytes, const char *what)
+int sddc::alloc(sddc_ctx *ctx, void **p, size_t bytes, const char *what)
 {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
     if (e != cudaSuccess) {
@@ -457,7 +393,7 @@ extern "C" int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, doub
     return SDDC_OK;
 }
 
-static StageArgs base_args(sddc_ctx *ctx)
+StageArgs sddc::base_args(sddc_ctx *ctx)
 {
     StageArgs a{};
     a.ncell = ctx->ncell;
@@ -488,7 +424,7 @@ static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a_in)
     }
 }
 
-static int ready(sddc_ctx *ctx)
+int sddc::ready(sddc_ctx *ctx)
 {
     if (!ctx) return SDDC_EINVAL;
     if (!ctx->tables) return set_err(ctx, SDDC_ESTATE, "tables not set (call sddc_set_tables)");
@@ -497,7 +433,7 @@ static int ready(sddc_ctx *ctx)
     return SDDC_OK;
 }
 
-static int check_flags(sddc_ctx *ctx)
+int sddc::check_flags(sddc_ctx *ctx)
 {
     CK(cudaMemcpyAsync(ctx->host_small, ctx->err_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

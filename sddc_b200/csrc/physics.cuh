@@ -17,12 +17,11 @@ namespace sddc {
 
 constexpr double kGam = 5.0 / 3.0;  // gam, setup2d.f90:67
 
-template <typename R> __device__ __forceinline__ R Sqrt(R x);
-template <> __device__ __forceinline__ double Sqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float Sqrt<float>(float x) { return sqrtf(x); }
-template <typename R> __device__ __forceinline__ R Abs(R x);
-template <> __device__ __forceinline__ double Abs<double>(double x) { return fabs(x); }
-template <> __device__ __forceinline__ float Abs<float>(float x) { return fabsf(x); }
+// overloads per arithmetic type (dual.cuh adds the dual-number ones)
+__device__ __forceinline__ double Sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float Sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double Abs(double x) { return fabs(x); }
+__device__ __forceinline__ float Abs(float x) { return fabsf(x); }
 template <typename R> __device__ __forceinline__ R Max(R a, R b) { return a > b ? a : b; }
 
 struct Freestream {
@@ -118,7 +117,7 @@ template <typename R, bool EX>
 __device__ __forceinline__ void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *Fnr, R n0, R n1, int sign_l,
                                         int sign_r, R c_h, R &eigv_out, R &umax)
 {
-    const R magnorm = Sqrt<R>(n0 * n0 + n1 * n1);
+    const R magnorm = Sqrt(n0 * n0 + n1 * n1);
     R unit_x, unit_y, ul, vl, wl, ur, vr, wr, pl, pr;
     const R Bxl = Qfl[5], Byl = Qfl[6], Bzl = Qfl[7], psil = Qfl[8];
     const R Bxr = Qfr[5], Byr = Qfr[6], Bzr = Qfr[7], psir = Qfr[8];
@@ -192,9 +191,9 @@ __device__ __forceinline__ void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *F
         c_n = (R)2 * bn * bn * rs;
     }
     const R cad = c_a + c_d;
-    const R c_tmp = Sqrt<R>(cad * cad - (R)4 * c_a * c_n);
-    const R c_f = Sqrt<R>((R)0.5 * ((c_a + c_d) + c_tmp));
-    const R eigv = (R)0.5 * Abs<R>(Vn_l + Vn_r) + c_f;
+    const R c_tmp = Sqrt(cad * cad - (R)4 * c_a * c_n);
+    const R c_f = Sqrt((R)0.5 * ((c_a + c_d) + c_tmp));
+    const R eigv = (R)0.5 * Abs(Vn_l + Vn_r) + c_f;
     const R sl = magnorm * (R)sign_l;
     const R slr = (R)(sign_l * sign_r);
 #pragma unroll
@@ -205,7 +204,7 @@ __device__ __forceinline__ void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *F
         Fnr[k] = slr * f;
     }
     eigv_out = eigv;
-    const R um = Max(Max((R)0.5 * Abs<R>(ul + ur), (R)0.5 * Abs<R>(vl + vr)), (R)0.5 * Abs<R>(wl + wr));
+    const R um = Max(Max((R)0.5 * Abs(ul + ur), (R)0.5 * Abs(vl + vr)), (R)0.5 * Abs(wl + wr));
     if (um > umax) umax = um;
 }
 
@@ -256,7 +255,7 @@ __device__ __forceinline__ void bc_ghost(int kind, const R *Qfl, R n0, R n1, int
         Qfr[7] = -Qfl[7];
         Qfr[8] = Qfl[8];
         if (vismode == 0) {
-            const R magnorm = Sqrt<R>(n0 * n0 + n1 * n1);
+            const R magnorm = Sqrt(n0 * n0 + n1 * n1);
             const R VN = uw * n0 / magnorm + vw * n1 / magnorm;
             Qfr[1] = rhow * (uw - (R)2 * VN * n0 / magnorm);
             Qfr[2] = rhow * (vw - (R)2 * VN * n1 / magnorm);
@@ -270,7 +269,7 @@ __device__ __forceinline__ void bc_ghost(int kind, const R *Qfl, R n0, R n1, int
         const R rhow = Qfl[0];
         const R uw = Qfl[1] / rhow, vw = Qfl[2] / rhow, ww = Qfl[3] / rhow;
         Qfr[0] = (R)fs.rinf * (R)2 - Qfl[0];
-        const R magnorm = Sqrt<R>(n0 * n0 + n1 * n1);
+        const R magnorm = Sqrt(n0 * n0 + n1 * n1);
         const R VN = uw * n0 / magnorm + vw * n1 / magnorm;
         Qfr[1] = Qfr[0] * (uw - (R)2 * VN * n0 / magnorm);
         Qfr[2] = Qfr[0] * (vw - (R)2 * VN * n1 / magnorm);

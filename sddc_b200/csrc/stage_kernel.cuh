@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         if (!(Ql[0] > (R)0) || !(Qr[0] > (R)0)) err |= kErrNonPositiveDensity;
         R eig_face;
         rusanov<R, EX>(Ql, Qr, Fl, Fr, n0, n1, sign_l, sign_r, c_h, eig_face, umax);
-        if (!(Abs<R>(eig_face) < (R)INFINITY)) err |= kErrNonFiniteWaveSpeed;
+        if (!(Abs(eig_face) < (R)INFINITY)) err |= kErrNonFiniteWaveSpeed;
         if (eig_face > eigmax) eigmax = eig_face;
 #pragma unroll
         for (int k = 0; k < 9; k++) slot[k] = own_right ? Fr[k] : Fl[k];
