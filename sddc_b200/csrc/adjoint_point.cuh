@@ -1,0 +1,350 @@
+// Reverse-mode (adjoint) point functions of the SDDC residual, by hand.
+//
+// Each function takes the adjoint of a point function's output and adds the
+// adjoint of its inputs (vector-Jacobian product):
+//   iflux_vjp     computational flux n0*F + n1*G at an interior flux point
+//                 (getIfluxvectors, getrusanov.f90:127-193)
+//   rusanov_vjp   Rusanov face flux of the left cell (getrusanovflux,
+//                 getrusanov.f90:1-125), with the wave speed and the face
+//                 velocity maximum as extra outputs
+//   bc_ghost_vjp  boundary ghost states (BCFLUX, bcflux.f90:17-375),
+//                 including the free-stream parameters
+// The primal values they recompute use the exact form's expressions, so that
+// the wave speed and velocity maximum they return equal, bit for bit, those
+// of the forward exact stage kernel (both are compiled with -fmad=false).
+// Non-smooth points take the branch the primal takes: |x| has slope +1 at
+// x == 0 (as fabs's branch x >= 0), max() the argument it returns, and the
+// square root of the fast-speed discriminant has slope 0 where the
+// discriminant is 0.
+#pragma once
+
+#include "physics.cuh"
+
+namespace sddc {
+
+constexpr double kG1 = kGam - 1.0;
+
+SDDC_HD double sgn1(double x) { return x < 0.0 ? -1.0 : 1.0; }
+
+// Adjoint of Fc = n0*F(Q, c) + n1*G(Q, c) at one interior flux point.
+// fb: adjoint of Fc; qb += (dFc/dQ)^T fb.  Returns fb . dFc/dc; um gets the
+// point's velocity maximum max(|u|, |v|, |w|) and um_d its gradient with
+// respect to Q (for the running-max adjoint).
+SDDC_HD double iflux_vjp(const double *Q, double c, double n0, double n1, const double *fb, double *qb, double &um,
+                         double *um_d)
+{
+    const double rho = Q[0], mx = Q[1], my = Q[2], mz = Q[3], E = Q[4];
+    const double Bx = Q[5], By = Q[6], Bz = Q[7], psi = Q[8];
+    // primal, exact-form velocity maximum
+    const double u = mx / rho, v = my / rho, w = mz / rho;
+    const double au = Abs(u), av = Abs(v), aw = Abs(w);
+    const double m1 = Max(au, av);
+    um = Max(m1, aw);
+    if (um_d) {
+        // the selected component: Max(a, b) returns b unless a > b
+        const int sel = (m1 > aw) ? (au > av ? 0 : 1) : 2;
+        const double comp = sel == 0 ? u : (sel == 1 ? v : w);
+        const double s = sgn1(comp) / rho;
+        for (int k = 0; k < 9; k++) um_d[k] = 0.0;
+        um_d[0] = -s * comp;
+        um_d[1 + sel] = s;
+    }
+    const double NB = (Bx * Bx + By * By) + Bz * Bz;
+    const double q2 = (u * u + v * v) + w * w;
+    const double pr = kG1 * (((E - 0.5 * rho * q2) - 0.5 * NB) - 0.5 * (psi * psi));
+    const double eb = ((E - 0.5 * (psi * psi)) + pr) + 0.5 * NB;
+    const double ub = (u * Bx + v * By) + w * Bz;
+
+    double a[9], b[9];
+    for (int k = 0; k < 9; k++) {
+        a[k] = n0 * fb[k];
+        b[k] = n1 * fb[k];
+    }
+    const double ebb = a[4] * u + b[4] * v;
+    const double ubb = -(a[4] * Bx + b[4] * By);
+    const double pb = a[1] + b[2] + ebb;
+    double ubar = a[0] * rho + 2.0 * a[1] * rho * u + a[2] * rho * v + a[3] * rho * w + a[4] * eb + ubb * Bx +
+                  a[6] * By + a[7] * Bz - b[5] * By + b[1] * rho * v;
+    double vbar = b[0] * rho + 2.0 * b[2] * rho * v + b[1] * rho * u + b[3] * rho * w + b[4] * eb + ubb * By -
+                  a[6] * Bx + b[5] * Bx + b[7] * Bz + a[2] * rho * u;
+    double wbar = a[3] * rho * u + b[3] * rho * v + ubb * Bz - a[7] * Bx - b[7] * By;
+    double rbar = a[0] * u + b[0] * v + a[1] * u * u + a[2] * u * v + a[3] * u * w + b[1] * u * v + b[2] * v * v +
+                  b[3] * v * w;
+    double Ebar = ebb;
+    double Bxb = -a[1] * Bx - a[2] * By - a[3] * Bz + a[4] * (c * psi - ub) - a[6] * v - a[7] * w + a[8] * c -
+                 b[1] * By + b[2] * Bx + b[5] * v + ubb * u + ebb * Bx;
+    double Byb = a[1] * By - a[2] * Bx + a[6] * u - b[1] * Bx - b[2] * By - b[3] * Bz + b[4] * (c * psi - ub) -
+                 b[5] * u - b[7] * w + b[8] * c + ubb * v + ebb * By;
+    double Bzb = a[1] * Bz - a[3] * Bx + a[7] * u + b[2] * Bz - b[3] * By + b[7] * v + ubb * w + ebb * Bz;
+    double psib = a[4] * c * Bx + a[5] * c + b[4] * c * By + b[6] * c - ebb * psi;
+    // pressure p = (gam-1) (E - rho |u|^2 / 2 - |B|^2 / 2 - psi^2 / 2)
+    Ebar += kG1 * pb;
+    rbar -= kG1 * 0.5 * q2 * pb;
+    ubar -= kG1 * rho * u * pb;
+    vbar -= kG1 * rho * v * pb;
+    wbar -= kG1 * rho * w * pb;
+    Bxb -= kG1 * Bx * pb;
+    Byb -= kG1 * By * pb;
+    Bzb -= kG1 * Bz * pb;
+    psib -= kG1 * psi * pb;
+    // primitive -> conserved
+    qb[0] += rbar - (ubar * u + vbar * v + wbar * w) / rho;
+    qb[1] += ubar / rho;
+    qb[2] += vbar / rho;
+    qb[3] += wbar / rho;
+    qb[4] += Ebar;
+    qb[5] += Bxb;
+    qb[6] += Byb;
+    qb[7] += Bzb;
+    qb[8] += psib;
+    return a[4] * psi * Bx + a[5] * psi + a[8] * Bx + b[4] * psi * By + b[6] * psi + b[8] * By;
+}
+
+// per-side quantities of the Rusanov flux
+struct RusSide {
+    double rho, mx, my, mz, E, Bx, By, Bz, psi;
+    double u, v, w, NB, p, pt, Vn, Bn, ub;
+};
+
+SDDC_HD void rus_side(const double *Q, double ux, double uy, RusSide &s)
+{
+    s.rho = Q[0]; s.mx = Q[1]; s.my = Q[2]; s.mz = Q[3]; s.E = Q[4];
+    s.Bx = Q[5]; s.By = Q[6]; s.Bz = Q[7]; s.psi = Q[8];
+    const double rhoi = 1.0 / s.rho;
+    s.u = rhoi * s.mx; s.v = rhoi * s.my; s.w = rhoi * s.mz;
+    s.NB = (s.Bx * s.Bx + s.By * s.By) + s.Bz * s.Bz;
+    s.p = kG1 * (((s.E - 0.5 * s.rho * ((s.u * s.u + s.v * s.v) + s.w * s.w)) - s.NB * 0.5) - 0.5 * (s.psi * s.psi));
+    s.pt = s.p + 0.5 * s.NB;
+    s.Vn = s.u * ux + s.v * uy;
+    s.Bn = s.Bx * ux + s.By * uy;
+    s.ub = (s.u * s.Bx + s.v * s.By) + s.w * s.Bz;
+}
+
+// adjoint of one side's normal flux Fn (a: adjoint of Fn, 9) plus the
+// adjoints that reach the side from the wave speed (Vnb, pgb) and the
+// averaged field (Bb) and density (rb), and from the face velocity maximum
+// (ubx: adjoint of u, v, w); adds the conserved-variable adjoint to qb
+SDDC_HD void rus_side_vjp(const RusSide &s, double c, double ux, double uy, const double *a, double Vnb, double pgb,
+                          const double *Bb, double rb, const double *uvwb, double *qb)
+{
+    Vnb += a[0] * s.rho + a[1] * s.mx + a[2] * s.my + a[3] * s.mz + a[4] * ((s.E - 0.5 * (s.psi * s.psi)) + s.pt) +
+           a[7] * s.Bz;
+    const double Bnb = -a[1] * s.Bx - a[2] * s.By - a[3] * s.Bz - a[4] * s.ub + a[4] * c * s.psi - a[7] * s.w + a[8] * c;
+    const double ptb = a[1] * ux + a[2] * uy + a[4] * s.Vn;
+    const double ubb = -a[4] * s.Bn;
+    double rhob = a[0] * s.Vn + rb;
+    double mxb = a[1] * s.Vn, myb = a[2] * s.Vn, mzb = a[3] * s.Vn;
+    double Eb = a[4] * s.Vn;
+    double psib = -a[4] * s.psi * s.Vn + a[4] * c * s.Bn + a[5] * c * ux + a[6] * c * uy;
+    double Bxb = -a[1] * s.Bn + a[5] * s.v * uy - a[6] * s.v * ux + Bb[0];
+    double Byb = -a[2] * s.Bn - a[5] * s.u * uy + a[6] * s.u * ux + Bb[1];
+    double Bzb = -a[3] * s.Bn + a[7] * s.Vn + Bb[2];
+    double ub = -a[5] * s.By * uy + a[6] * s.By * ux + uvwb[0];
+    double vb = a[5] * s.Bx * uy - a[6] * s.Bx * ux + uvwb[1];
+    double wb = -a[7] * s.Bn + uvwb[2];
+    // Vn = u ux + v uy, Bn = Bx ux + By uy, ub = u.B
+    ub += Vnb * ux + ubb * s.Bx;
+    vb += Vnb * uy + ubb * s.By;
+    wb += ubb * s.Bz;
+    Bxb += Bnb * ux + ubb * s.u;
+    Byb += Bnb * uy + ubb * s.v;
+    Bzb += ubb * s.w;
+    // pt = p + |B|^2/2 and pg = pt - |B|^2/2 (= p): the field terms cancel
+    // for the wave speed's pg
+    const double pb = ptb + pgb;
+    Bxb += ptb * s.Bx;
+    Byb += ptb * s.By;
+    Bzb += ptb * s.Bz;
+    // p = (gam-1) (E - rho |u|^2 / 2 - |B|^2 / 2 - psi^2 / 2)
+    Eb += kG1 * pb;
+    rhob -= kG1 * 0.5 * ((s.u * s.u + s.v * s.v) + s.w * s.w) * pb;
+    ub -= kG1 * s.rho * s.u * pb;
+    vb -= kG1 * s.rho * s.v * pb;
+    wb -= kG1 * s.rho * s.w * pb;
+    Bxb -= kG1 * s.Bx * pb;
+    Byb -= kG1 * s.By * pb;
+    Bzb -= kG1 * s.Bz * pb;
+    psib -= kG1 * s.psi * pb;
+    // u = mx / rho
+    qb[0] += rhob - (ub * s.u + vb * s.v + wb * s.w) / s.rho;
+    qb[1] += mxb + ub / s.rho;
+    qb[2] += myb + vb / s.rho;
+    qb[3] += mzb + wb / s.rho;
+    qb[4] += Eb;
+    qb[5] += Bxb;
+    qb[6] += Byb;
+    qb[7] += Bzb;
+    qb[8] += psib;
+}
+
+// Adjoint of the Rusanov flux f (the left cell's computational flux; the
+// right cell's is sign_l*sign_r*f) with respect to both traces.
+// fb: adjoint of f; eb0, umb0: extra adjoints of the wave speed and of the
+// face velocity maximum.  qlb, qrb accumulate.  eig and um return the primal
+// wave speed and velocity maximum (exact form).
+SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double c,
+                         const double *fb, double eb0, double umb0, double *qlb, double *qrb, double &eig, double &um)
+{
+    const double magnorm = Sqrt(n0 * n0 + n1 * n1);
+    const double ux = n0 / magnorm * (double)sign_l;
+    const double uy = n1 / magnorm * (double)sign_l;
+    RusSide L, R;
+    rus_side(Ql, ux, uy, L);
+    rus_side(Qr, ux, uy, R);
+    // wave speed of the averaged state (exact-form expressions)
+    const double pgl = L.pt - 0.5 * L.NB, pgr = R.pt - 0.5 * R.NB;
+    const double Bx = 0.5 * (L.Bx + R.Bx), By = 0.5 * (L.By + R.By), Bz = 0.5 * (L.Bz + R.Bz);
+    const double bn = Bx * ux + By * uy;
+    const double S = L.rho + R.rho;
+    const double ca = kGam * (pgl + pgr) / S;
+    const double cd = ((Bx * Bx + By * By) + Bz * Bz) / (0.5 * S);
+    const double cn = bn * bn / (0.5 * S);
+    const double cad = ca + cd;
+    const double ct = Sqrt(cad * cad - 4.0 * ca * cn);
+    const double cf = Sqrt(0.5 * ((ca + cd) + ct));
+    const double vs = L.Vn + R.Vn;
+    eig = 0.5 * Abs(vs) + cf;
+    const double xu = 0.5 * Abs(L.u + R.u), xv = 0.5 * Abs(L.v + R.v), xw = 0.5 * Abs(L.w + R.w);
+    const double m1 = Max(xu, xv);
+    um = Max(m1, xw);
+    const int usel = (m1 > xw) ? (xu > xv ? 0 : 1) : 2;
+
+    // f_k = K ((Fnl_k + Fnr_k) - eig (Qr_k - Ql_k)), K = |n| sign_l / 2
+    const double K = 0.5 * magnorm * (double)sign_l;
+    double g[9], ebar = eb0;
+    for (int k = 0; k < 9; k++) {
+        g[k] = K * fb[k];
+        ebar -= g[k] * (Qr[k] - Ql[k]);
+        qlb[k] += eig * g[k];
+        qrb[k] -= eig * g[k];
+    }
+    // eig = |Vnl + Vnr| / 2 + cf
+    const double Vnb = 0.5 * sgn1(vs) * ebar;
+    const double cfb = ebar;
+    const double cadb0 = cfb * 0.25 / cf;
+    const double ctb = cfb * 0.25 / cf;
+    const double Db = ct > 0.0 ? ctb * 0.5 / ct : 0.0;
+    const double cadb = cadb0 + 2.0 * cad * Db;
+    const double cab = -4.0 * cn * Db + cadb;
+    const double cnb = -4.0 * ca * Db;
+    const double cdb = cadb;
+    const double pgb = cab * kGam / S;
+    double Sb = -cab * ca / S - cdb * cd / S - cnb * cn / S;
+    const double bnb = cnb * 4.0 * bn / S;
+    double Bh[3] = {cdb * 4.0 * Bx / S + bnb * ux, cdb * 4.0 * By / S + bnb * uy, cdb * 4.0 * Bz / S};
+    const double Bhalf[3] = {0.5 * Bh[0], 0.5 * Bh[1], 0.5 * Bh[2]};
+    // face velocity maximum: max over (|ul+ur|, |vl+vr|, |wl+wr|) / 2
+    double uvwl[3] = {0.0, 0.0, 0.0}, uvwr[3] = {0.0, 0.0, 0.0};
+    {
+        const double comp = usel == 0 ? L.u + R.u : (usel == 1 ? L.v + R.v : L.w + R.w);
+        const double d = 0.5 * sgn1(comp) * umb0;
+        uvwl[usel] = d;
+        uvwr[usel] = d;
+    }
+    rus_side_vjp(L, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwl, qlb);
+    rus_side_vjp(R, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwr, qrb);
+}
+
+// d f_k / d c_h of the Rusanov flux (nonzero for k = 4, 5, 6, 8)
+SDDC_HD void rusanov_dfdc(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double *d)
+{
+    const double magnorm = Sqrt(n0 * n0 + n1 * n1);
+    const double ux = n0 / magnorm * (double)sign_l;
+    const double uy = n1 / magnorm * (double)sign_l;
+    const double K = 0.5 * magnorm * (double)sign_l;
+    const double Bnl = Ql[5] * ux + Ql[6] * uy, Bnr = Qr[5] * ux + Qr[6] * uy;
+    const double ps = Ql[8] + Qr[8];
+    for (int k = 0; k < 9; k++) d[k] = 0.0;
+    d[4] = K * (Ql[8] * Bnl + Qr[8] * Bnr);
+    d[5] = K * ps * ux;
+    d[6] = K * ps * uy;
+    d[8] = K * (Bnl + Bnr);
+}
+
+// d (n0 F_k + n1 G_k) / d c_h at an interior flux point
+SDDC_HD void iflux_dfdc(const double *Q, double n0, double n1, double *d)
+{
+    for (int k = 0; k < 9; k++) d[k] = 0.0;
+    d[4] = Q[8] * (Q[5] * n0 + Q[6] * n1);
+    d[5] = Q[8] * n0;
+    d[6] = Q[8] * n1;
+    d[8] = Q[5] * n0 + Q[6] * n1;
+}
+
+// Adjoint of the boundary ghost state Qr = ghost(Ql, free stream).
+// qrb: adjoint of Qr; qlb += (dQr/dQl)^T qrb; pb (rinf, pinf, uinf, vinf,
+// bxinf, byinf) += (dQr/dfs)^T qrb.
+SDDC_HD void bc_ghost_vjp(int kind, const double *Ql, double n0, double n1, int vismode, const Freestream &fs,
+                          const double *qrb, double *qlb, double *pb)
+{
+    if (kind == kFaceInle) {
+        const double rr = fs.rinf, ur = fs.uinf, vr = fs.vinf;
+        qlb[8] += qrb[8] + qrb[4] * Ql[8];
+        pb[0] += qrb[0] + qrb[1] * ur + qrb[2] * vr + qrb[4] * 0.5 * (ur * ur + vr * vr);
+        pb[2] += qrb[1] * rr + qrb[4] * rr * ur;
+        pb[3] += qrb[2] * rr + qrb[4] * rr * vr;
+        pb[1] += qrb[4] / kG1;
+        pb[4] += qrb[5] + qrb[4] * fs.bxinf;
+        pb[5] += qrb[6] + qrb[4] * fs.byinf;
+    } else if (kind == kFaceOutl) {
+        const double rl = Ql[0], ur = Ql[1] / rl, vr = Ql[2] / rl;
+        const double rrb = qrb[0] + qrb[1] * ur + qrb[2] * vr + qrb[4] * 0.5 * (ur * ur + vr * vr);
+        const double urb = qrb[1] * rl + qrb[4] * rl * ur;
+        const double vrb = qrb[2] * rl + qrb[4] * rl * vr;
+        qlb[0] += rrb - (urb * ur + vrb * vr) / rl;
+        qlb[1] += urb / rl;
+        qlb[2] += vrb / rl;
+        qlb[8] += qrb[4] * Ql[8];
+        pb[1] += qrb[4] / kG1;
+        pb[4] += qrb[5] + qrb[4] * fs.bxinf;
+        pb[5] += qrb[6] + qrb[4] * fs.byinf;
+    } else if (kind == kFaceWall) {
+        qlb[0] += qrb[0];
+        qlb[4] += qrb[4];
+        qlb[5] -= qrb[5];
+        qlb[6] -= qrb[6];
+        qlb[7] -= qrb[7];
+        qlb[8] += qrb[8];
+        qlb[3] -= qrb[3];
+        if (vismode == 0) {  // slip: reflected normal momentum
+            const double m = Sqrt(n0 * n0 + n1 * n1);
+            const double h0 = n0 / m, h1 = n1 / m;
+            qlb[1] += qrb[1] * (1.0 - 2.0 * h0 * h0) - 2.0 * h0 * h1 * qrb[2];
+            qlb[2] += -2.0 * h0 * h1 * qrb[1] + (1.0 - 2.0 * h1 * h1) * qrb[2];
+        } else {  // no-slip: momentum negated
+            qlb[1] -= qrb[1];
+            qlb[2] -= qrb[2];
+        }
+    } else if (kind == kFaceSymp) {
+        const double rl = Ql[0];
+        const double uw = Ql[1] / rl, vw = Ql[2] / rl, ww = Ql[3] / rl;
+        const double rr = fs.rinf * 2.0 - rl;
+        const double m = Sqrt(n0 * n0 + n1 * n1);
+        const double h0 = n0 / m, h1 = n1 / m;
+        const double VN = uw * h0 + vw * h1;
+        const double uh = uw - 2.0 * VN * h0, vh = vw - 2.0 * VN * h1, wh = -ww;
+        const double Q1 = rr * uh, Q2 = rr * vh, Q3 = rr * wh;
+        const double Q1b = qrb[1] + qrb[4] * Q1 / rr;
+        const double Q2b = qrb[2] + qrb[4] * Q2 / rr;
+        const double Q3b = qrb[3] + qrb[4] * Q3 / rr;
+        const double rrb = qrb[0] - qrb[4] * 0.5 * ((Q1 * Q1 + Q2 * Q2) + Q3 * Q3) / (rr * rr) + Q1b * uh + Q2b * vh +
+                           Q3b * wh;
+        const double uhb = rr * Q1b, vhb = rr * Q2b, whb = rr * Q3b;
+        const double VNb = -2.0 * (uhb * h0 + vhb * h1);
+        const double uwb = uhb + VNb * h0, vwb = vhb + VNb * h1, wwb = -whb;
+        qlb[1] += uwb / rl;
+        qlb[2] += vwb / rl;
+        qlb[3] += wwb / rl;
+        qlb[0] += -(uwb * uw + vwb * vw + wwb * ww) / rl - rrb;
+        qlb[7] += -qrb[7] + qrb[4] * Ql[7];
+        qlb[8] += qrb[8] + qrb[4] * Ql[8];
+        pb[0] += 2.0 * rrb;
+        pb[1] += qrb[4] / kG1;
+        pb[4] += qrb[5] + qrb[4] * fs.bxinf;
+        pb[5] += qrb[6] + qrb[4] * fs.byinf;
+    } else {  // FREE: copy
+        for (int k = 0; k < 9; k++) qlb[k] += qrb[k];
+    }
+}
+
+}  // namespace sddc

@@ -17,12 +17,14 @@ namespace sddc {
 
 constexpr double kGam = 5.0 / 3.0;  // gam, setup2d.f90:67
 
-// overloads per arithmetic type (dual.cuh adds the dual-number ones)
-__device__ __forceinline__ double Sqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float Sqrt(float x) { return sqrtf(x); }
-__device__ __forceinline__ double Abs(double x) { return fabs(x); }
-__device__ __forceinline__ float Abs(float x) { return fabsf(x); }
-template <typename R> __device__ __forceinline__ R Max(R a, R b) { return a > b ? a : b; }
+#define SDDC_HD __host__ __device__ __forceinline__
+
+// overloads per arithmetic type (a test's dual-number type adds its own)
+SDDC_HD double Sqrt(double x) { return sqrt(x); }
+SDDC_HD float Sqrt(float x) { return sqrtf(x); }
+SDDC_HD double Abs(double x) { return fabs(x); }
+SDDC_HD float Abs(float x) { return fabsf(x); }
+template <typename R> SDDC_HD R Max(R a, R b) { return a > b ? a : b; }
 
 struct Freestream {
     double rinf, pinf, uinf, vinf, bxinf, byinf;
@@ -32,7 +34,7 @@ struct Freestream {
 // done in FP64, where the cancellation of E against the kinetic, magnetic and
 // psi energies (low plasma beta) costs no digits beyond the inputs'.
 template <typename R>
-__device__ __forceinline__ R pressure_fast(const R *q, R rinv)
+SDDC_HD R pressure_fast(const R *q, R rinv)
 {
     const double rho_i = (double)rinv;
     const double m2 = (double)q[1] * q[1] + (double)q[2] * q[2] + (double)q[3] * q[3];
@@ -44,7 +46,7 @@ __device__ __forceinline__ R pressure_fast(const R *q, R rinv)
 // getIfluxvectors, getrusanov.f90:127-193: F and G at one flux point,
 // and the running max of |u|,|v|,|w|.
 template <typename R, bool EX>
-__device__ __forceinline__ void iflux(const R *Q, R c_h, R &umax, R *F, R *G)
+SDDC_HD void iflux(const R *Q, R c_h, R &umax, R *F, R *G)
 {
     const R rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoE = Q[4];
     const R Bx = Q[5], By = Q[6], Bz = Q[7], psi = Q[8];
@@ -114,7 +116,7 @@ __device__ __forceinline__ void iflux(const R *Q, R c_h, R &umax, R *F, R *G)
 // computational flux in Fnl, the right cell's in Fnr and the wave speed in
 // eigv; updates the running max of the face-averaged velocity.
 template <typename R, bool EX>
-__device__ __forceinline__ void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *Fnr, R n0, R n1, int sign_l,
+SDDC_HD void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *Fnr, R n0, R n1, int sign_l,
                                         int sign_r, R c_h, R &eigv_out, R &umax)
 {
     const R magnorm = Sqrt(n0 * n0 + n1 * n1);
@@ -222,7 +224,7 @@ enum FaceKind : int {
 
 // Boundary ghost states of BCFLUX (bcflux.f90:17-375).
 template <typename R, bool EX>
-__device__ __forceinline__ void bc_ghost(int kind, const R *Qfl, R n0, R n1, int vismode, const Freestream &fs,
+SDDC_HD void bc_ghost(int kind, const R *Qfl, R n0, R n1, int vismode, const Freestream &fs,
                                          R *Qfr)
 {
     const R gm1 = (R)(kGam - 1.0);
