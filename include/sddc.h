@@ -198,6 +198,62 @@ int sddc_compresid_noalloc(const sddc_params *p, const double *Lmat, const doubl
                            double eigvmax, double umax, double *resid_dev, double *nablaqs_dev,
                            double *maxima_out, void *stream);
 
+/* ---- discrete adjoint -------------------------------------------------------
+   The VJP of the FP64 residual and of RK_S5P3 time stepping.  The reference
+   has no adjoint; these entries are the "sddc_vjp_resid" and
+   "sddc_adjoint_run" that a Fortran or Python caller binds beside
+   compresid (compresid.f90:1-80) and RK_S5P3 (iterations.f90:158-213).
+   The residual differentiated is the exact FP64 form's (bit-equal to the
+   reference's) whatever precision the context runs; the AV sensor enters no
+   residual (its coefficients are zero, getrusanov.f90:326,328) and has no
+   adjoint.  c_h = sqrt(L (L - U)) depends on the running maxima L, U of the
+   wave speed and velocity over all earlier stages; its adjoint goes to the
+   points attaining each maximum, split equally among them when several
+   attain it bit for bit (a shared face counted once), to the first stage
+   that attained it.  |x| has slope +1 at 0 and max() follows the argument
+   it returns.  Single case (no batch), mu = eta0 = 0, k_stage = 3. */
+
+/* Qbar = (dR/dQ)^T Rbar at the current state, with R as sddc_compresid
+   evaluates it (c_h from the running maxima now held).  Host arrays
+   (9,N,N,NCELL).  parbar (nullable) gets 7 values: Rbar . dR/dc_h, then
+   Rbar . dR/d(rinf, pinf, uinf, vinf, bxinf, byinf) through the boundary
+   states.  The context's state and maxima are unchanged. */
+int sddc_vjp_resid(sddc_ctx *ctx, const double *Rbar, double *Qbar, double *parbar);
+
+typedef struct sddc_adjoint_opts {
+    double dt;              /* RK_S5P3 time step */
+    int nsteps;             /* steps run from the current state */
+    int n1, n2;             /* objective window: states after n1..n2 steps, 0 <= n1 <= n2 <= nsteps */
+    double w_drag, w_lift;  /* J = mean over the window of w_drag*C_D + w_lift*C_L */
+    double diameter;        /* reference length D of C = 2F/(rho_inf |U_inf|^2 D); 0 means 1 */
+    int checkpoint_every;   /* steps between stored states (0 means 20) */
+} sddc_adjoint_opts;
+
+typedef struct sddc_adjoint_stats {
+    double forward_ms;    /* the recorded forward run */
+    double reverse_ms;    /* recomputation and reverse sweep */
+    double device_bytes;  /* device memory the run allocated (checkpoints, stage states, adjoints) */
+    int owner_stages;     /* stages whose wave-speed or velocity maximum raised the running max */
+    int tie_stages;       /* of those, stages where several points attained it */
+} sddc_adjoint_stats;
+
+/* Drag and lift are not in the reference.  The force on the wall faces is
+   F = sum over IBFWAL face points of w * (momentum components of the wall
+   face's Rusanov flux out of the fluid), w the solution-point quadrature
+   weight along the face; C_D and C_L are its components along the free
+   stream (uinf, vinf) and normal to it, times 2/(rho_inf |U_inf|^2 D).
+   Runs nsteps exact FP64 RK_S5P3 steps from the current state and running
+   maxima, recording a checkpoint every checkpoint_every steps; obj
+   (nullable) gets J, mean C_D, mean C_L over the window.  With Qbar0 or
+   parbar non-null, then runs the reverse sweep (recomputing each segment
+   from its checkpoint): Qbar0 (9,N,N,NCELL) = dJ/dQ(initial state), parbar
+   (6) = dJ/d(rinf, pinf, uinf, vinf, bxinf, byinf) through the boundary
+   states, the normalisation of C held fixed.  The context ends at the final
+   state and maxima, as after sddc_rk_step(ctx, dt, nsteps) in the exact
+   form.  stats is nullable. */
+int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *opts, double *obj, double *Qbar0, double *parbar,
+                     sddc_adjoint_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,8 @@ CUDA_UNITS = {
     "stage_mixed.cu": [],
     "context.cu": [],
     "noalloc.cu": [],
-    "adjoint.cu": ["-fmad=false"],
+    "adjoint.cu": [],
+    "adjoint_exact.cu": ["-fmad=false"],
 }
 
 

@@ -9,10 +9,9 @@
 //                 velocity maximum as extra outputs
 //   bc_ghost_vjp  boundary ghost states (BCFLUX, bcflux.f90:17-375),
 //                 including the free-stream parameters
-// The primal values they recompute use the exact form's expressions, so that
-// the wave speed and velocity maximum they return equal, bit for bit, those
-// of the forward exact stage kernel (both are compiled with -fmad=false).
-// Non-smooth points take the branch the primal takes: |x| has slope +1 at
+// They recompute the primal values they need with reciprocals (the argmax of
+// a running maximum is located by the forward's own point functions, so
+// these need not round as the forward does).  Non-smooth points take the branch the primal takes: |x| has slope +1 at
 // x == 0 (as fabs's branch x >= 0), max() the argument it returns, and the
 // square root of the fast-speed discriminant has slope 0 where the
 // discriminant is 0.
@@ -35,8 +34,8 @@ SDDC_HD double iflux_vjp(const double *Q, double c, double n0, double n1, const 
 {
     const double rho = Q[0], mx = Q[1], my = Q[2], mz = Q[3], E = Q[4];
     const double Bx = Q[5], By = Q[6], Bz = Q[7], psi = Q[8];
-    // primal, exact-form velocity maximum
-    const double u = mx / rho, v = my / rho, w = mz / rho;
+    const double ri = 1.0 / rho;
+    const double u = mx * ri, v = my * ri, w = mz * ri;
     const double au = Abs(u), av = Abs(v), aw = Abs(w);
     const double m1 = Max(au, av);
     um = Max(m1, aw);
@@ -44,7 +43,7 @@ SDDC_HD double iflux_vjp(const double *Q, double c, double n0, double n1, const 
         // the selected component: Max(a, b) returns b unless a > b
         const int sel = (m1 > aw) ? (au > av ? 0 : 1) : 2;
         const double comp = sel == 0 ? u : (sel == 1 ? v : w);
-        const double s = sgn1(comp) / rho;
+        const double s = sgn1(comp) * ri;
         for (int k = 0; k < 9; k++) um_d[k] = 0.0;
         um_d[0] = -s * comp;
         um_d[1 + sel] = s;
@@ -88,10 +87,10 @@ SDDC_HD double iflux_vjp(const double *Q, double c, double n0, double n1, const 
     Bzb -= kG1 * Bz * pb;
     psib -= kG1 * psi * pb;
     // primitive -> conserved
-    qb[0] += rbar - (ubar * u + vbar * v + wbar * w) / rho;
-    qb[1] += ubar / rho;
-    qb[2] += vbar / rho;
-    qb[3] += wbar / rho;
+    qb[0] += rbar - (ubar * u + vbar * v + wbar * w) * ri;
+    qb[1] += ubar * ri;
+    qb[2] += vbar * ri;
+    qb[3] += wbar * ri;
     qb[4] += Ebar;
     qb[5] += Bxb;
     qb[6] += Byb;
@@ -103,15 +102,15 @@ SDDC_HD double iflux_vjp(const double *Q, double c, double n0, double n1, const 
 // per-side quantities of the Rusanov flux
 struct RusSide {
     double rho, mx, my, mz, E, Bx, By, Bz, psi;
-    double u, v, w, NB, p, pt, Vn, Bn, ub;
+    double ri, u, v, w, NB, p, pt, Vn, Bn, ub;
 };
 
 SDDC_HD void rus_side(const double *Q, double ux, double uy, RusSide &s)
 {
     s.rho = Q[0]; s.mx = Q[1]; s.my = Q[2]; s.mz = Q[3]; s.E = Q[4];
     s.Bx = Q[5]; s.By = Q[6]; s.Bz = Q[7]; s.psi = Q[8];
-    const double rhoi = 1.0 / s.rho;
-    s.u = rhoi * s.mx; s.v = rhoi * s.my; s.w = rhoi * s.mz;
+    s.ri = 1.0 / s.rho;
+    s.u = s.ri * s.mx; s.v = s.ri * s.my; s.w = s.ri * s.mz;
     s.NB = (s.Bx * s.Bx + s.By * s.By) + s.Bz * s.Bz;
     s.p = kG1 * (((s.E - 0.5 * s.rho * ((s.u * s.u + s.v * s.v) + s.w * s.w)) - s.NB * 0.5) - 0.5 * (s.psi * s.psi));
     s.pt = s.p + 0.5 * s.NB;
@@ -166,10 +165,10 @@ SDDC_HD void rus_side_vjp(const RusSide &s, double c, double ux, double uy, cons
     Bzb -= kG1 * s.Bz * pb;
     psib -= kG1 * s.psi * pb;
     // u = mx / rho
-    qb[0] += rhob - (ub * s.u + vb * s.v + wb * s.w) / s.rho;
-    qb[1] += mxb + ub / s.rho;
-    qb[2] += myb + vb / s.rho;
-    qb[3] += mzb + wb / s.rho;
+    qb[0] += rhob - (ub * s.u + vb * s.v + wb * s.w) * s.ri;
+    qb[1] += mxb + ub * s.ri;
+    qb[2] += myb + vb * s.ri;
+    qb[3] += mzb + wb * s.ri;
     qb[4] += Eb;
     qb[5] += Bxb;
     qb[6] += Byb;
@@ -178,87 +177,90 @@ SDDC_HD void rus_side_vjp(const RusSide &s, double c, double ux, double uy, cons
 }
 
 // Adjoint of the Rusanov flux f (the left cell's computational flux; the
-// right cell's is sign_l*sign_r*f) with respect to both traces.
+// right cell's is sign_l*sign_r*f) with respect to the traces.
 // fb: adjoint of f; eb0, umb0: extra adjoints of the wave speed and of the
-// face velocity maximum.  qlb, qrb accumulate.  eig and um return the primal
-// wave speed and velocity maximum (exact form).
+// face velocity maximum.  qlb, qrb accumulate; either may be null (that
+// side's adjoint is not formed).  eig and um return the wave speed and
+// velocity maximum; dfdc (nullable) gets d f / d c_h.
 SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double c,
-                         const double *fb, double eb0, double umb0, double *qlb, double *qrb, double &eig, double &um)
+                         const double *fb, double eb0, double umb0, double *qlb, double *qrb, double &eig, double &um,
+                         double *dfdc = nullptr)
 {
     const double magnorm = Sqrt(n0 * n0 + n1 * n1);
-    const double ux = n0 / magnorm * (double)sign_l;
-    const double uy = n1 / magnorm * (double)sign_l;
-    RusSide L, R;
-    rus_side(Ql, ux, uy, L);
-    rus_side(Qr, ux, uy, R);
-    // wave speed of the averaged state (exact-form expressions)
-    const double pgl = L.pt - 0.5 * L.NB, pgr = R.pt - 0.5 * R.NB;
-    const double Bx = 0.5 * (L.Bx + R.Bx), By = 0.5 * (L.By + R.By), Bz = 0.5 * (L.Bz + R.Bz);
-    const double bn = Bx * ux + By * uy;
-    const double S = L.rho + R.rho;
-    const double ca = kGam * (pgl + pgr) / S;
-    const double cd = ((Bx * Bx + By * By) + Bz * Bz) / (0.5 * S);
-    const double cn = bn * bn / (0.5 * S);
+    const double sm = (double)sign_l / magnorm;
+    const double ux = n0 * sm, uy = n1 * sm;
+    // the quantities both sides share
+    double Vn_s, pg[2], rho[2], Bh[3], uvw[3], Bn[2];
+    for (int sd = 0; sd < 2; sd++) {
+        RusSide S;
+        rus_side(sd == 0 ? Ql : Qr, ux, uy, S);
+        pg[sd] = S.p;
+        rho[sd] = S.rho;
+        Bn[sd] = S.Bn;
+        if (sd == 0) {
+            Vn_s = S.Vn;
+            Bh[0] = S.Bx; Bh[1] = S.By; Bh[2] = S.Bz;
+            uvw[0] = S.u; uvw[1] = S.v; uvw[2] = S.w;
+        } else {
+            Vn_s += S.Vn;
+            Bh[0] = 0.5 * (Bh[0] + S.Bx); Bh[1] = 0.5 * (Bh[1] + S.By); Bh[2] = 0.5 * (Bh[2] + S.Bz);
+            uvw[0] += S.u; uvw[1] += S.v; uvw[2] += S.w;
+        }
+    }
+    const double K = 0.5 * magnorm * (double)sign_l;
+    if (dfdc) {
+        const double ps = Ql[8] + Qr[8];
+        for (int k = 0; k < 9; k++) dfdc[k] = 0.0;
+        dfdc[4] = K * (Ql[8] * Bn[0] + Qr[8] * Bn[1]);
+        dfdc[5] = K * ps * ux;
+        dfdc[6] = K * ps * uy;
+        dfdc[8] = K * (Bn[0] + Bn[1]);
+    }
+    const double bn = Bh[0] * ux + Bh[1] * uy;
+    const double S = rho[0] + rho[1], iS = 1.0 / S;
+    const double ca = kGam * (pg[0] + pg[1]) * iS;
+    const double cd = 2.0 * ((Bh[0] * Bh[0] + Bh[1] * Bh[1]) + Bh[2] * Bh[2]) * iS;
+    const double cn = 2.0 * bn * bn * iS;
     const double cad = ca + cd;
     const double ct = Sqrt(cad * cad - 4.0 * ca * cn);
-    const double cf = Sqrt(0.5 * ((ca + cd) + ct));
-    const double vs = L.Vn + R.Vn;
-    eig = 0.5 * Abs(vs) + cf;
-    const double xu = 0.5 * Abs(L.u + R.u), xv = 0.5 * Abs(L.v + R.v), xw = 0.5 * Abs(L.w + R.w);
+    const double cf = Sqrt(0.5 * (cad + ct));
+    eig = 0.5 * Abs(Vn_s) + cf;
+    const double xu = 0.5 * Abs(uvw[0]), xv = 0.5 * Abs(uvw[1]), xw = 0.5 * Abs(uvw[2]);
     const double m1 = Max(xu, xv);
     um = Max(m1, xw);
     const int usel = (m1 > xw) ? (xu > xv ? 0 : 1) : 2;
 
     // f_k = K ((Fnl_k + Fnr_k) - eig (Qr_k - Ql_k)), K = |n| sign_l / 2
-    const double K = 0.5 * magnorm * (double)sign_l;
-    double g[9], ebar = eb0;
-    for (int k = 0; k < 9; k++) {
-        g[k] = K * fb[k];
-        ebar -= g[k] * (Qr[k] - Ql[k]);
-        qlb[k] += eig * g[k];
-        qrb[k] -= eig * g[k];
-    }
+    double ebar = eb0;
+    for (int k = 0; k < 9; k++) ebar -= K * fb[k] * (Qr[k] - Ql[k]);
     // eig = |Vnl + Vnr| / 2 + cf
-    const double Vnb = 0.5 * sgn1(vs) * ebar;
-    const double cfb = ebar;
-    const double cadb0 = cfb * 0.25 / cf;
-    const double ctb = cfb * 0.25 / cf;
-    const double Db = ct > 0.0 ? ctb * 0.5 / ct : 0.0;
-    const double cadb = cadb0 + 2.0 * cad * Db;
+    const double Vnb = 0.5 * sgn1(Vn_s) * ebar;
+    const double q4 = 0.25 * ebar / cf;  // d eig / d cad = d eig / d ct
+    const double Db = ct > 0.0 ? 0.5 * q4 / ct : 0.0;
+    const double cadb = q4 + 2.0 * cad * Db;
     const double cab = -4.0 * cn * Db + cadb;
     const double cnb = -4.0 * ca * Db;
     const double cdb = cadb;
-    const double pgb = cab * kGam / S;
-    double Sb = -cab * ca / S - cdb * cd / S - cnb * cn / S;
-    const double bnb = cnb * 4.0 * bn / S;
-    double Bh[3] = {cdb * 4.0 * Bx / S + bnb * ux, cdb * 4.0 * By / S + bnb * uy, cdb * 4.0 * Bz / S};
-    const double Bhalf[3] = {0.5 * Bh[0], 0.5 * Bh[1], 0.5 * Bh[2]};
+    const double pgb = cab * kGam * iS;
+    const double Sb = -(cab * ca + cdb * cd + cnb * cn) * iS;
+    const double bnb = 4.0 * cnb * bn * iS;
+    const double c4 = 2.0 * cdb * iS;  // half of d cd / d Bh
+    const double Bhalf[3] = {c4 * Bh[0] + 0.5 * bnb * ux, c4 * Bh[1] + 0.5 * bnb * uy, c4 * Bh[2]};
     // face velocity maximum: max over (|ul+ur|, |vl+vr|, |wl+wr|) / 2
-    double uvwl[3] = {0.0, 0.0, 0.0}, uvwr[3] = {0.0, 0.0, 0.0};
-    {
-        const double comp = usel == 0 ? L.u + R.u : (usel == 1 ? L.v + R.v : L.w + R.w);
-        const double d = 0.5 * sgn1(comp) * umb0;
-        uvwl[usel] = d;
-        uvwr[usel] = d;
+    double uvwb[3] = {0.0, 0.0, 0.0};
+    uvwb[usel] = 0.5 * sgn1(uvw[usel]) * umb0;
+    double g[9];
+    for (int k = 0; k < 9; k++) g[k] = K * fb[k];
+    for (int sd = 0; sd < 2; sd++) {
+        double *qb = sd == 0 ? qlb : qrb;
+        if (!qb) continue;
+        const double *Q = sd == 0 ? Ql : Qr;
+        const double sg = sd == 0 ? eig : -eig;
+        for (int k = 0; k < 9; k++) qb[k] += sg * g[k];
+        RusSide Sd;
+        rus_side(Q, ux, uy, Sd);
+        rus_side_vjp(Sd, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwb, qb);
     }
-    rus_side_vjp(L, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwl, qlb);
-    rus_side_vjp(R, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwr, qrb);
-}
-
-// d f_k / d c_h of the Rusanov flux (nonzero for k = 4, 5, 6, 8)
-SDDC_HD void rusanov_dfdc(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double *d)
-{
-    const double magnorm = Sqrt(n0 * n0 + n1 * n1);
-    const double ux = n0 / magnorm * (double)sign_l;
-    const double uy = n1 / magnorm * (double)sign_l;
-    const double K = 0.5 * magnorm * (double)sign_l;
-    const double Bnl = Ql[5] * ux + Ql[6] * uy, Bnr = Qr[5] * ux + Qr[6] * uy;
-    const double ps = Ql[8] + Qr[8];
-    for (int k = 0; k < 9; k++) d[k] = 0.0;
-    d[4] = K * (Ql[8] * Bnl + Qr[8] * Bnr);
-    d[5] = K * ps * ux;
-    d[6] = K * ps * uy;
-    d[8] = K * (Bnl + Bnr);
 }
 
 // d (n0 F_k + n1 G_k) / d c_h at an interior flux point

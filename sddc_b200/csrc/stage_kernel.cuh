@@ -102,6 +102,7 @@ struct StageArgs {
     double *__restrict__ resid_out;    // (9,N,N,NCELL), residual evaluation only
     double *__restrict__ grad_out;     // (9,2,N,N,NCELL), residual evaluation only
     double *__restrict__ mon_part;     // per-CTA (sum resid^2, sum divB^2), or null
+    double *__restrict__ cta_max;      // per-CTA (max eigv, max umax) of this stage, or null
     unsigned *err_flags;
 };
 
@@ -678,6 +679,10 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             if (a.mon_part) {
                 a.mon_part[2 * blockIdx.x] = s0;
                 a.mon_part[2 * blockIdx.x + 1] = s1;
+            }
+            if (a.cta_max) {  // where the running maxima were raised (the adjoint's argmax)
+                a.cta_max[2 * blockIdx.x] = m0;
+                a.cta_max[2 * blockIdx.x + 1] = m1;
             }
         }
     }

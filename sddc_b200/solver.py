@@ -32,7 +32,7 @@ OK, EINVAL, ECUDA, ESTATE, ENUMERIC, ENOMEM = 0, -1, -2, -3, -4, -5
 EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables", "sddc_set_state",
             "sddc_compresid", "sddc_rk_step", "sddc_get_state", "sddc_monitor", "sddc_get_maxima",
             "sddc_state_device_ptr", "sddc_get_stream", "sddc_set_cases", "sddc_rk_step_cases",
-            "sddc_get_case_maxima")
+            "sddc_get_case_maxima", "sddc_vjp_resid", "sddc_adjoint_run")
 
 
 class Params(ctypes.Structure):
@@ -46,6 +46,18 @@ class CaseRecord(ctypes.Structure):
     """sddc_case: one case of a batch."""
     _fields_ = [("first_cell", _I), ("ncell", _I), ("dt", _D), ("rinf", _D), ("pinf", _D), ("uinf", _D),
                 ("vinf", _D), ("bxinf", _D), ("byinf", _D)]
+
+
+class AdjointOpts(ctypes.Structure):
+    """sddc_adjoint_opts."""
+    _fields_ = [("dt", _D), ("nsteps", _I), ("n1", _I), ("n2", _I), ("w_drag", _D), ("w_lift", _D),
+                ("diameter", _D), ("checkpoint_every", _I)]
+
+
+class AdjointStats(ctypes.Structure):
+    """sddc_adjoint_stats."""
+    _fields_ = [("forward_ms", _D), ("reverse_ms", _D), ("device_bytes", _D), ("owner_stages", _I),
+                ("tie_stages", _I)]
 
 
 class SddcError(RuntimeError):
@@ -78,6 +90,9 @@ def lib():
         L.sddc_set_cases.argtypes = [ctypes.c_void_p, _I, ctypes.POINTER(CaseRecord)]
         L.sddc_rk_step_cases.argtypes = [ctypes.c_void_p, _I]
         L.sddc_get_case_maxima.argtypes = [ctypes.c_void_p, _I, _PD, _PD]
+        L.sddc_vjp_resid.argtypes = [ctypes.c_void_p, _PD, _PD, _PD]
+        L.sddc_adjoint_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(AdjointOpts), _PD, _PD, _PD,
+                                       ctypes.POINTER(AdjointStats)]
         L._sddc_typed = True
     return L
 
@@ -219,6 +234,35 @@ class Solver:
         e, u = _D(), _D()
         self._check(self._L.sddc_get_case_maxima(self._h, int(icase), ctypes.byref(e), ctypes.byref(u)))
         return e.value, u.value
+
+    # -- discrete adjoint -----------------------------------------------------
+    def vjp_resid(self, Rbar):
+        """(dR/dQ)^T Rbar at the current state (exact FP64 residual); returns
+        (Qbar, parbar) with parbar = [Rbar . dR/dc_h, Rbar . dR/d(rinf, pinf,
+        uinf, vinf, bxinf, byinf)]."""
+        Rbar = np.asfortranarray(Rbar, dtype=np.float64)
+        Qbar = np.zeros((9, self.N, self.N, self.ncell), order="F")
+        par = np.zeros(7)
+        self._check(self._L.sddc_vjp_resid(self._h, ptr(Rbar), ptr(Qbar), ptr(par)))
+        return Qbar, par
+
+    def adjoint_run(self, dt, nsteps, n1, n2, w_drag=1.0, w_lift=0.0, diameter=1.0, checkpoint_every=20,
+                    gradient=True):
+        """nsteps exact RK_S5P3 steps from the current state and the
+        objective J = mean over the states after n1..n2 steps of
+        w_drag*C_D + w_lift*C_L, with (gradient=True) dJ/dQ0 and dJ/d(free
+        stream) by the discrete adjoint.  The context ends at the final
+        state."""
+        o = AdjointOpts(dt=dt, nsteps=int(nsteps), n1=int(n1), n2=int(n2), w_drag=w_drag, w_lift=w_lift,
+                        diameter=diameter, checkpoint_every=int(checkpoint_every))
+        obj = np.zeros(3)
+        st = AdjointStats()
+        Qbar = np.zeros((9, self.N, self.N, self.ncell), order="F") if gradient else None
+        par = np.zeros(6) if gradient else None
+        self._check(self._L.sddc_adjoint_run(self._h, ctypes.byref(o), ptr(obj), ptr(Qbar) if gradient else None,
+                                             ptr(par) if gradient else None, ctypes.byref(st)))
+        return dict(J=obj[0], cd=obj[1], cl=obj[2], Qbar0=Qbar, parbar=par,
+                    stats={f: getattr(st, f) for f, _ in AdjointStats._fields_})
 
     # -- the reference's time loop -------------------------------------------
     def iterations(self, dt, maxiter, resid_out=None, iter0=0, ncellglob=None):

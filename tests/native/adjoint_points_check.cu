@@ -63,7 +63,7 @@ int main()
             report("iflux <w,Jv>", fwd, rev, scale);
             m_iflux = std::fmax(m_iflux, std::fabs(fwd - rev) / scale);
             report("iflux um", um.d[0], umdir, std::fabs(um.d[0]) + 1.0);
-            if (um.v != umv) { std::printf("  iflux um value differs\n"); worst = 1.0; }
+            report("iflux um value", um.v, umv, um.v + 1e-300);
             // c derivative
             for (int k = 0; k < 9; k++) Q[k] = D1(q[k]);
             D1 cc(c);
@@ -94,26 +94,25 @@ int main()
             rusanov<D1, true>(Ql, Qr, Fl, Fr, D1(n0), D1(n1), sl, sr, D1(c), eig, um);
             double fwd = eb0 * eig.d[0] + umb0 * um.d[0], scale = std::fabs(eb0 * eig.d[0]) + std::fabs(umb0 * um.d[0]);
             for (int k = 0; k < 9; k++) { fwd += fb[k] * Fl[k].d[0]; scale += std::fabs(fb[k] * Fl[k].d[0]); }
-            double qlb[9] = {0}, qrb[9] = {0}, eigv, umv;
-            rusanov_vjp(ql, qr, n0, n1, sl, c, fb, eb0, umb0, qlb, qrb, eigv, umv);
+            double qlb[9] = {0}, qrb[9] = {0}, eigv, umv, dfdc[9];
+            rusanov_vjp(ql, qr, n0, n1, sl, c, fb, eb0, umb0, qlb, qrb, eigv, umv, dfdc);
             double rev = 0.0;
             for (int k = 0; k < 9; k++) rev += qlb[k] * vl[k] + qrb[k] * vr[k];
             report("rusanov <w,Jv>", fwd, rev, scale);
             m_rus = std::fmax(m_rus, std::fabs(fwd - rev) / scale);
-            // primal values equal the double exact form's bit for bit
+            // primal values agree with the exact form to rounding
             double dl[9], dr[9], Fld[9], Frd[9], e2, u2 = 0.0;
             for (int k = 0; k < 9; k++) { dl[k] = ql[k]; dr[k] = qr[k]; }
             rusanov<double, true>(dl, dr, Fld, Frd, n0, n1, sl, sr, c, e2, u2);
-            if (e2 != eigv || u2 != umv) { std::printf("  rusanov primal differs\n"); worst = 1.0; }
+            report("rusanov eig", e2, eigv, e2);
+            report("rusanov um", u2, umv, u2 + 1e-300);
             // c derivative
             for (int k = 0; k < 9; k++) { Ql[k] = D1(ql[k]); Qr[k] = D1(qr[k]); }
             D1 cc(c);
             cc.d[0] = 1.0;
             D1 um3(0.0);
             rusanov<D1, true>(Ql, Qr, Fl, Fr, D1(n0), D1(n1), sl, sr, cc, eig, um3);
-            double d[9];
-            rusanov_dfdc(ql, qr, n0, n1, sl, d);
-            for (int k = 0; k < 9; k++) report("rusanov dfdc", Fl[k].d[0], d[k], std::fabs(Fl[k].d[0]) + 1.0);
+            for (int k = 0; k < 9; k++) report("rusanov dfdc", Fl[k].d[0], dfdc[k], std::fabs(Fl[k].d[0]) + 1.0);
         }
         // ---- boundary ghost states --------------------------------------------
         {
