@@ -294,6 +294,8 @@ def run_ours(args):
                 "steps": e2e_steps, "path": "sddc_set_state + sddc_rk_step + sddc_get_state + sddc_monitor"},
         "gpu_launches": 5 * steps,
         "ensemble": ensemble_run(torch) if not args.no_ensemble else None,
+        "adjoint": adjoint_bench(torch, nsteps=args.adjoint_steps, n1=args.adjoint_steps * 5 // 6,
+                                 n2=args.adjoint_steps) if args.adjoint_steps else None,
     }
     print(json.dumps(line))
     if dist:
@@ -388,6 +390,78 @@ def ensemble_run(torch, ncase=64, steps=20, warmup=3, seed=0):
             "batched_over_sequential": t_seq / t_batch}
 
 
+def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
+    """The discrete adjoint on the cylinder 128x256, p = 3 (N = 4): the
+    objective is C_D averaged over the states after n1..n2 exact RK_S5P3
+    steps; gradients with respect to the initial field and the inflow sonic
+    and Alfven Mach numbers (through the boundary states and the initial
+    field), checkpoints every 20 steps.  Cost ratio: the reverse sweep
+    (recomputation and VJPs) over the plain exact forward run of the same
+    steps, both timed with CUDA events on the context's stream.  A few
+    central differences (h = 1e-6) of J check the gradient."""
+    from sddc_b200 import adjoint, cases, host, mesh
+    from sddc_b200.solver import Solver
+
+    m = mesh.cylinder_ogrid(128, 256)
+    t = host.build_tables(m, 4)
+    ph = cases.cylinder_physics(ms=MS, ma=MA)
+    Q0 = cases.freestream_state(ph, 4, m.ncell, noise=1e-6, seed=seed)
+    dt = cases.cfl_dt(m, Q0, 4)
+    free0 = torch.cuda.mem_get_info()[0]
+    prob = adjoint.DragLiftProblem(t, dt, nsteps, n1, n2, w_drag=1.0, w_lift=0.0, checkpoint_every=20)
+    fs0 = np.array([ph.rinf, ph.pinf, ph.uinf, ph.vinf, ph.bxinf, ph.byinf])
+    s = prob.solver(fs0)
+    ctx_bytes = free0 - torch.cuda.mem_get_info()[0]
+    # the plain forward of the same steps (exact form, graph-launched)
+    s.set_state(Q0)
+    s.rk_s5p3(dt, 3)
+    s.set_state(Q0)
+    st = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.rk_s5p3(dt, nsteps)
+    e1.record(st)
+    e1.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    # objective and gradients (Mach numbers through the boundary states and Q0)
+    fs_base = adjoint.cylinder_freestream(MS, MA).numpy()
+    Qbase = adjoint.freestream_field(torch.from_numpy(fs_base), 4, m.ncell).numpy()
+    noise = Q0 - Qbase
+    J, dms, dma, qbar = adjoint.mach_gradients(prob, MS, MA, noise)
+    r = prob.last
+    # central differences of J in random directions of the initial field; the
+    # running max behind c_h makes J piecewise smooth, so a step that moves
+    # the argmax of one of the thousands of raised maxima averages the
+    # one-sided slopes: both a 1e-6 and a 1e-9 step are reported
+    rng = np.random.default_rng(seed + 1)
+    scale = np.abs(Q0).max(axis=(1, 2, 3), keepdims=True)
+    errs = {1e-6: [], 1e-9: []}
+    Q0b = Qbase + noise
+    for _ in range(fd_dirs):
+        V = rng.uniform(-1.0, 1.0, Q0.shape) * scale
+        ad = float(np.vdot(qbar, V))
+        for h in errs:
+            jp = prob.run(Q0b + h * V, fs_base, gradient=False)["J"]
+            jm = prob.run(Q0b - h * V, fs_base, gradient=False)["J"]
+            errs[h].append(abs((jp - jm) / (2 * h) - ad) / max(abs(ad), 1e-300))
+    prob.close()
+    stats = r["stats"]
+    return {"workload": "cylinder O-grid 128x256, p=3 (N=4), exact FP64 RK_S5P3, "
+                        f"{nsteps} steps, J = mean C_D over steps {n1}..{n2}, checkpoints every 20 steps",
+            "J": J, "cd": r["cd"], "cl": r["cl"], "dJ_dMs": dms, "dJ_dMA": dma,
+            "dJ_dQ0_l2": float(np.linalg.norm(qbar)),
+            "forward_ms": fwd_ms, "recording_forward_ms": stats["forward_ms"], "reverse_ms": stats["reverse_ms"],
+            "cost_ratio": stats["reverse_ms"] / fwd_ms,
+            "cost_ratio_with_recording": (stats["forward_ms"] + stats["reverse_ms"]) / fwd_ms,
+            "owner_stages": stats["owner_stages"], "stages": 5 * nsteps,
+            "device_bytes_run": stats["device_bytes"], "device_bytes_context": int(ctx_bytes),
+            "fd_check": {"directions": fd_dirs,
+                         "max_rel_err_h1e-6": max(errs[1e-6]) if fd_dirs else None,
+                         "max_rel_err_h1e-9": max(errs[1e-9]) if fd_dirs else None},
+            "tangent_check": "tests/test_gpu_adjoint.py: adjoint = complex-step FP64 CPU tangent to 1e-12 "
+                             "(24x48 cells, 200 steps, 600 raised maxima)"}
+
+
 def cpu_baseline(t, ph, Q0, dt, dof, steps=1):
     """The CPU oracle on all host threads, one RK3 step of the full mesh."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -451,6 +525,8 @@ def main():
                     help="time one form only (the command used for ncu captures)")
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="RK3 steps of the mixed/FP64 vs FP64-exact comparison (0: skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=1200,
+                    help="RK3 steps of the discrete-adjoint block (objective over the last sixth; 0: skip)")
     ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8, 16],
                     help="cells per CTA; 0 lets the autotuner choose")
     args = ap.parse_args()

@@ -166,3 +166,90 @@ def test_adjoint_central_differences():
         ad = float(np.vdot(r["Qbar0"], V))
         assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3), (trial, fd, ad)
     s.close()
+
+
+def _cs_field(ms, ma, noise):
+    """The cylinder free-stream field plus noise, in complex arithmetic."""
+    p = 1.0 / (cases.GAMMA * ms * ms)
+    bx = 1.0 / ma
+    q = np.array([1.0, 1.0, 0.0, 0.0, p / (cases.GAMMA - 1.0) + 0.5 + 0.5 * bx * bx, bx, 0.0, 0.0, 0.0],
+                 dtype=np.complex128)
+    return np.asfortranarray(q[:, None, None, None] + noise), np.array([1.0, p, 1.0, 0.0, bx, 0.0],
+                                                                       dtype=np.complex128)
+
+
+@pytest.mark.gpu
+def test_torch_function_mach_gradients():
+    """dJ/dMs and dJ/dMA through the autograd wrapper (boundary states and
+    initial field) against the complex-step tangent of the oracle's run."""
+    from sddc_b200 import adjoint
+    m, t, ph, _ = case_cylinder(6, 12, 4)
+    ms, ma = 0.5, 2.0
+    noise = np.random.default_rng(4).uniform(-1e-3, 1e-3, (9, t.N, t.N, t.ncell))
+    Qr, _ = _cs_field(ms, ma, noise)
+    dt = cases.cfl_dt(m, Qr.real.copy(order="F"), t.N)
+    nsteps, n1, n2, wd, wl = 12, 4, 12, 1.0, 0.5
+    prob = adjoint.DragLiftProblem(t, dt, nsteps, n1, n2, w_drag=wd, w_lift=wl, checkpoint_every=5)
+    J, dms, dma, _ = adjoint.mach_gradients(prob, ms, ma, noise)
+    prob.close()
+    phys = cases.cylinder_physics(ms, ma)
+    for which, ad in (("ms", dms), ("ma", dma)):
+        Qc, fsc = _cs_field(ms + (1j * H if which == "ms" else 0), ma + (1j * H if which == "ma" else 0), noise)
+        Jt, _ = _oracle_objective(t, phys, Qc, dt, nsteps, n1, n2, wd, wl, tangent=True, fs=fsc)
+        assert abs(Jt.real - J) <= 1e-12 * abs(J)
+        d_tan = Jt.imag / H
+        assert abs(d_tan - ad) <= 1e-9 * (abs(d_tan) + 1e-12), (which, d_tan, ad)
+
+
+@pytest.mark.gpu
+def test_adjoint_long_run_matches_tangent():
+    """200 steps on a 24x48 cylinder (hundreds of stages raise a running
+    maximum): the adjoint equals the complex-step tangent to rounding."""
+    import os
+    O.set_threads(os.cpu_count() or 1)
+    from sddc_b200 import host, mesh
+    m = mesh.cylinder_ogrid(24, 48)
+    t = host.build_tables(m, 4)
+    ph = cases.cylinder_physics(ms=0.5, ma=2.0)
+    Q0 = cases.freestream_state(ph, 4, m.ncell, noise=1e-6, seed=0)
+    dt = cases.cfl_dt(m, Q0, 4)
+    nsteps, n1 = 200, 150
+    s = Solver(t, ph, precision="fp64_exact")
+    s.set_state(Q0)
+    r = s.adjoint_run(dt, nsteps, n1, nsteps, w_drag=1.0, w_lift=0.25)
+    s.close()
+    assert r["stats"]["owner_stages"] > 100
+    V = np.random.default_rng(1).uniform(-1, 1, Q0.shape) * np.abs(Q0).max(axis=(1, 2, 3), keepdims=True)
+    Jt, _ = _oracle_objective(t, ph, Q0 + 1j * H * V, dt, nsteps, n1, nsteps, 1.0, 0.25, tangent=True)
+    d_tan, d_adj = Jt.imag / H, float(np.vdot(r["Qbar0"], V))
+    assert abs(d_tan - d_adj) <= 1e-12 * abs(d_tan), (d_tan, d_adj)
+
+
+@pytest.mark.gpu
+def test_adjoint_fullsize_central_differences():
+    """The configured adjoint case (cylinder 128x256, p = 3, C_D over steps
+    1000-1200): 16 seeded directions of the initial field against central
+    differences with h = 1e-9 (below the spacing of the running-max kinks,
+    above rounding; a 1e-6 step crosses kinks of the max-based c_h)."""
+    from sddc_b200 import host, mesh
+    m = mesh.cylinder_ogrid(128, 256)
+    t = host.build_tables(m, 4)
+    ph = cases.cylinder_physics(ms=0.5, ma=2.0)
+    Q0 = cases.freestream_state(ph, 4, m.ncell, noise=1e-6, seed=0)
+    dt = cases.cfl_dt(m, Q0, 4)
+    s = Solver(t, ph, precision="fp64_exact")
+    s.set_state(Q0)
+    r = s.adjoint_run(dt, 1200, 1000, 1200, w_drag=1.0)
+    rng = np.random.default_rng(16)
+    scale = np.abs(Q0).max(axis=(1, 2, 3), keepdims=True)
+    h, worst = 1e-9, 0.0
+    for _ in range(16):
+        V = rng.uniform(-1, 1, Q0.shape) * scale
+        js = []
+        for sg in (1, -1):
+            s.set_state(Q0 + sg * h * V)
+            js.append(s.adjoint_run(dt, 1200, 1000, 1200, w_drag=1.0, gradient=False)["J"])
+        ad = float(np.vdot(r["Qbar0"], V))
+        worst = max(worst, abs((js[0] - js[1]) / (2 * h) - ad) / abs(ad))
+    s.close()
+    assert worst < 1e-5, worst
