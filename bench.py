@@ -456,8 +456,12 @@ def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
             "owner_stages": stats["owner_stages"], "stages": 5 * nsteps,
             "device_bytes_run": stats["device_bytes"], "device_bytes_context": int(ctx_bytes),
             "fd_check": {"directions": fd_dirs,
-                         "max_rel_err_h1e-6": max(errs[1e-6]) if fd_dirs else None,
-                         "max_rel_err_h1e-9": max(errs[1e-9]) if fd_dirs else None},
+                         "h1e-6": {"max_rel_err": max(errs[1e-6]), "median_rel_err": float(np.median(errs[1e-6]))}
+                         if fd_dirs else None,
+                         "h1e-9": {"max_rel_err": max(errs[1e-9]), "median_rel_err": float(np.median(errs[1e-9]))}
+                         if fd_dirs else None,
+                         "note": "h=1e-6 crosses kinks of the running-max c_h; at h=1e-9 the rounding of J "
+                                 "over 1200 steps limits the quotient to ~1e-5"},
             "tangent_check": "tests/test_gpu_adjoint.py: adjoint = complex-step FP64 CPU tangent to 1e-12 "
                              "(24x48 cells, 200 steps, 600 raised maxima)"}
 
