@@ -22,6 +22,7 @@ max over ranks and ``value`` is the total over ranks.
 from __future__ import annotations
 
 import argparse
+import math
 import json
 import os
 import statistics
@@ -148,6 +149,18 @@ def time_form(torch, solver_mod, t, ph, Q0, dt, precision, steps, warmup):
     return s, ms
 
 
+def max_over_ranks(dist, x: float, device: str = "cuda") -> float:
+    """The largest of every rank's x (identity on one process).  Every rank
+    must call it at the same point: it is a collective."""
+    if dist is None:
+        return x
+    import torch
+
+    m = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return float(m.item())
+
+
 def run_ours(args):
     import torch
 
@@ -198,10 +211,7 @@ def run_ours(args):
             clocks = ck.summary()
         else:
             s, ms = time_form(torch, solver_mod, t, ph, Q0, dt, prec, steps, warm)
-        if dist:
-            m = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-            ms = float(m.item())
+        ms = max_over_ranks(dist, ms)
         results[prec] = ms
         states[prec] = s.state()["Q"]
         s.close()
@@ -229,10 +239,7 @@ def run_ours(args):
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     s.close()
-    if dist:
-        m = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        e2e_ms = float(m.item())
+    e2e_ms = max_over_ranks(dist, e2e_ms)
     if rank != 0:
         if dist:
             dist.barrier()
@@ -245,7 +252,9 @@ def run_ours(args):
         "after_steps": steps + warm,
         "note": "fp64_exact is bit-equal to the CPU oracle (tests/test_gpu_parity.py, test_gpu_fullsize.py)",
     }
-    if args.accuracy_steps:
+    # the single-GPU diagnostic blocks run at N = 1 only (replicas repeat them)
+    single = world == 1
+    if args.accuracy_steps and single:
         acc["long_run"] = accuracy_run(solver_mod, t, ph, Q0, dt, dof, args.accuracy_steps)
     units = dof * 5 * steps
     val = {k: world * units / (v / 1e3) for k, v in results.items()}
@@ -257,7 +266,7 @@ def run_ours(args):
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
         traffic = json.load(open(prof)).get("mixed_n5_bytes_per_launch")
-    cpu = cpu_baseline(t, ph, Q0, dt, dof) if not args.no_cpu_baseline else None
+    cpu = cpu_baseline(t, ph, Q0, dt, dof) if not args.no_cpu_baseline and single else None
     e2e_units = dof * 5 * e2e_steps * world
     line = {
         "metric": METRIC,
@@ -293,9 +302,9 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(Q0.nbytes), "d2h_bytes_per_step": int(Q0.nbytes) + 32,
                 "steps": e2e_steps, "path": "sddc_set_state + sddc_rk_step + sddc_get_state + sddc_monitor"},
         "gpu_launches": 5 * steps,
-        "ensemble": ensemble_run(torch) if not args.no_ensemble else None,
+        "ensemble": ensemble_run(torch) if not args.no_ensemble and single else None,
         "adjoint": adjoint_bench(torch, nsteps=args.adjoint_steps, n1=args.adjoint_steps * 5 // 6,
-                                 n2=args.adjoint_steps) if args.adjoint_steps else None,
+                                 n2=args.adjoint_steps) if args.adjoint_steps and single else None,
     }
     print(json.dumps(line))
     if dist:
@@ -330,6 +339,66 @@ def accuracy_run(solver_mod, t, ph, Q0, dt, dof, nsteps):
             "divB_l2": float(np.sqrt(mon["divbsum"] / dof)),
             "mass_change_minus_exact": (mon["mass"] - m0p) / m0p - res["mass_change_fp64_exact"],
         }
+    return res
+
+
+def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200):
+    """The Orszag-Tang vortex on a periodic 1024^2 mesh, p = 3, to t = 0.5
+    (dt fixed from CFL 0.3 of the initial state): each form from the same
+    seeded initial state, its DOF-stage/s (CUDA events on the context's
+    stream), and the mixed and FP64 forms' error against the exact FP64 form
+    (bit-equal to the CPU oracle) at the end: per-variable rel-L2, ||divB||,
+    mass drift.  A form that faults numerically reports the time reached."""
+    from sddc_b200 import cases, host
+    from sddc_b200.solver import NumericalFault, Solver
+
+    c = cases.config3(n)
+    t = host.build_tables(c.mesh, c.N)
+    Q0 = c.initial_state(t)
+    dt = cases.cfl_dt(c.mesh, Q0, c.N)
+    nsteps = int(math.ceil(t_end / dt))
+    dof = c.mesh.ncell * c.N * c.N
+    out, res = {}, {"workload": f"Orszag-Tang {n}x{n} periodic, p=3 (N=4), RK_S5P3, CFL 0.3, t_end={t_end}",
+                    "dof": dof, "dt": dt, "steps": nsteps}
+    for prec in ("fp64_exact", "fp64", "mixed"):
+        s = Solver(t, c.physics, precision=prec)
+        s.set_state(Q0)
+        m0 = s.monitor()["mass"]
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        done, fault, ms = 0, None, 0.0
+        while done < nsteps:
+            k = min(chunk, nsteps - done)
+            e0.record(st)
+            try:
+                s.rk_s5p3(dt, k)
+            except NumericalFault as e:
+                fault = str(e)
+                break
+            e1.record(st)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            done += k
+        mon = s.monitor() if fault is None else None
+        out[prec] = (s.state()["Q"] if fault is None else None, m0, mon)
+        res[prec] = {"steps_done": done, "t_reached": done * dt, "fault": fault,
+                     "value": dof * 5 * done / (ms / 1e3) if ms > 0 else None, "unit": UNIT}
+        s.close()
+    ref, m0, mref = out["fp64_exact"]
+    names = ["rho", "rhou", "rhov", "rhow", "E", "Bx", "By", "Bz", "psi"]
+    if ref is not None:
+        res["fp64_exact"].update(divB_l2=float(np.sqrt(mref["divbsum"] / dof)),
+                                 mass_change=(mref["mass"] - m0) / m0)
+        for prec in ("fp64", "mixed"):
+            q, m0p, mon = out[prec]
+            if q is None:
+                continue
+            res[prec].update(
+                rel_l2_all=float(np.linalg.norm(q - ref) / np.linalg.norm(ref)),
+                rel_l2_per_var={nm: float(np.linalg.norm(q[k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))
+                                for k, nm in enumerate(names)},
+                divB_l2=float(np.sqrt(mon["divbsum"] / dof)),
+                mass_change_minus_exact=(mon["mass"] - m0p) / m0p - res["fp64_exact"]["mass_change"])
     return res
 
 
@@ -533,11 +602,27 @@ def main():
                     help="RK3 steps of the discrete-adjoint block (objective over the last sixth; 0: skip)")
     ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8, 16],
                     help="cells per CTA; 0 lets the autotuner choose")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the discrete-adjoint block (with --adjoint-steps; the command profiled under ncu)")
+    ap.add_argument("--orszag-tang", action="store_true",
+                    help="run only the Orszag-Tang 1024^2 comparison (mixed/FP64 vs exact FP64 to t = 0.5)")
     args = ap.parse_args()
     global FIXED_TILE
     FIXED_TILE = args.tile
     if args.warmup < 3:
         args.warmup = 3
+    if args.adjoint_only:
+        import torch
+
+        n = args.adjoint_steps
+        print(json.dumps({"adjoint": adjoint_bench(torch, nsteps=n, n1=n * 5 // 6, n2=n,
+                                                   fd_dirs=3 if n >= 100 else 0)}))
+        return
+    if args.orszag_tang:
+        import torch
+
+        print(json.dumps({"orszag_tang": orszag_tang_run(torch)}))
+        return
     if args.impl == "reference":
         if args.steps > 10:
             args.steps = 10  # each step is a full CPU RK3 step of 3.3M points

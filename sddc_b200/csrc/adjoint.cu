@@ -542,10 +542,10 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
         std::memcpy(&acc, w->host, sizeof(AdjScalars));
         if (parbar)
             for (int m = 0; m < 6; m++) parbar[m] = acc.pbar[m];
+        ties = (int)acc.ties;
         CKA(cudaEventElapsedTime(&rev_ms, ev[1], ev[2]));
         if ((rc = adjoint_flags(ctx))) return rc;
     }
-    (void)ties;
     float fwd_ms = 0.0f;
     CKA(cudaEventElapsedTime(&fwd_ms, ev[0], ev[1]));
     if (stats) {
@@ -553,7 +553,7 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
         stats->reverse_ms = rev_ms;
         stats->device_bytes = (double)(rb.bytes + w->bytes);
         stats->owner_stages = owners;
-        stats->tie_stages = 0;
+        stats->tie_stages = ties;
     }
 
     // ---- the context continues from the final state -------------------------------

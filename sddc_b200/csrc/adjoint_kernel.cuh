@@ -48,7 +48,7 @@ struct AdjScalars {
     double lam_eig, lam_um;  // adjoints of the running maxima not yet given to their argmax
     double pbar[6];          // adjoint of (rinf, pinf, uinf, vinf, bxinf, byinf)
     double cbar;             // sum over stages of lambda . dR/dc_h
-    double pad;
+    double ties;             // stages whose raised maximum several points attained
 };
 
 struct VjpArgs {
@@ -600,6 +600,7 @@ static __global__ void __launch_bounds__(kRedThreads) adj_reduce_kernel(int nblk
         const double cb = t[0];
         for (int m = 0; m < 6; m++) acc->pbar[m] += t[1 + m] + ps[m];
         acc->cbar += cb;
+        if ((owner_eig && rec_cnt[0] > 1) || (owner_um && rec_cnt[1] > 1)) acc->ties += 1.0;
         acc->lam_eig = (owner_eig ? 0.0 : acc->lam_eig) + cb * dc_dl;
         acc->lam_um = (owner_um ? 0.0 : acc->lam_um) + cb * dc_du;
         *rec_n = 0;
