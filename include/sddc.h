@@ -58,14 +58,17 @@ typedef struct sddc_params {
     int k_stage;    /* 3: RK_S5P3, 5: FiveStageRk                              */
     int precision;  /* SDDC_FP64_EXACT, SDDC_FP64 or SDDC_MIXED                */
     int cells_per_cta; /* 0: default tile; else 4, 8 or 16 cells per CTA       */
-    double mu, eta0;   /* viscosity and resistivity; nonzero is rejected (see below) */
+    double mu, eta0;   /* viscosity and resistivity (QUAD.INP), >= 0            */
     double dxcycl, dycycl;
     double rinf, pinf, uinf, vinf, bxinf, byinf; /* free stream (QUAD.INP) */
 } sddc_params;
 
-/* Creates a context on the current CUDA device.  mu and eta0 must be 0:
-   with them zero the reference's viscous chain (compflux.f90:13-31) adds
-   exactly +0.0 to the residual, and this drop-in skips it. */
+/* Creates a context on the current CUDA device.  With vismode = 1 and mu
+   or eta0 nonzero every stage runs the reference's viscous / resistive
+   chain (compflux.f90:36-50: nablaQsp, gradient averaging, BCVISFLUX with
+   the adiabatic-wall energy gradient, getVfluxvectors) before the stage;
+   with both zero that chain adds exactly +0.0 to the residual and is
+   skipped.  Batches (sddc_set_cases) and the adjoint need mu = eta0 = 0. */
 int sddc_create(sddc_ctx **out, const sddc_params *p);
 void sddc_destroy(sddc_ctx *ctx);
 const char *sddc_last_error(const sddc_ctx *ctx);

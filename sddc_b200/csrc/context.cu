@@ -17,6 +17,7 @@
 
 #include "context_impl.h"
 #include "sd_basis.h"
+#include "visc_kernel.cuh"
 
 using namespace sddc;
 
@@ -165,7 +166,8 @@ static void free_all(sddc_ctx *ctx)
     for (auto &t : ctx->trace) cudaFree(t), t = nullptr;
     void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
                     ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags,
-                    ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag};
+                    ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag, ctx->visc_grad, ctx->visc_gt,
+                    ctx->visc_rv, ctx->met2};
     for (void *b : bufs) cudaFree(b);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     adjoint_free(ctx);
@@ -206,8 +208,7 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
     if (p->vismode != 0 && p->vismode != 1) return bad("vismode must be 0 or 1");
     if (p->k_stage != 3 && p->k_stage != 5) return bad("k_stage can be only 3 or 5 (iterations.f90:22-31)");
     if (p->precision < SDDC_FP64_EXACT || p->precision > SDDC_MIXED) return bad("unknown precision");
-    if (p->mu != 0.0 || p->eta0 != 0.0)
-        return bad("mu and eta0 must be 0: the viscous/resistive chain is not part of this drop-in");
+    if (!(p->mu >= 0.0) || !(p->eta0 >= 0.0)) return bad("mu and eta0 must be non-negative");
     if (p->cells_per_cta != 0 && p->cells_per_cta != 4 && p->cells_per_cta != 8 && p->cells_per_cta != 16)
         return bad("cells_per_cta must be 0, 4, 8 or 16");
     ctx->N = p->N;
@@ -240,6 +241,15 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
         (rc = alloc(ctx, (void **)&ctx->wq, kMaxN * sizeof(double), "weights")) ||
         (rc = alloc(ctx, (void **)&ctx->err_flags, sizeof(unsigned), "flags")))
         return rc;
+    // the viscous chain runs only with vismode = 1 (compflux.f90:36)
+    ctx->visc = p->vismode == 1 && (p->mu != 0.0 || p->eta0 != 0.0);
+    if (ctx->visc) {
+        if ((rc = alloc(ctx, (void **)&ctx->visc_grad, 2 * ctx->nq * sizeof(double), "viscous gradients")) ||
+            (rc = alloc(ctx, (void **)&ctx->visc_gt, nc * 4 * p->N * 18 * sizeof(double), "gradient traces")) ||
+            (rc = alloc(ctx, (void **)&ctx->visc_rv, ctx->nq * sizeof(double), "viscous residual")) ||
+            (rc = alloc(ctx, (void **)&ctx->met2, nc * 4 * p->N * 2 * sizeof(double), "face metrics")))
+            return rc;
+    }
     CK(cudaMallocHost((void **)&ctx->host_small, 64 * sizeof(double)));
     CK(cudaMemsetAsync(ctx->maxima, 0, kSlots * 2 * sizeof(double), ctx->stream));
     CK(cudaMemsetAsync(ctx->err_flags, 0, sizeof(unsigned), ctx->stream));
@@ -346,6 +356,36 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
                 break;
             }
     if (!msg.empty()) return set_err(ctx, SDDC_EINVAL, "sddc_set_tables: " + msg);
+    std::vector<double> met2;
+    if (ctx->visc) {
+        // the normal row the adiabatic-wall gradient state reads
+        // (bcflux.f90:527-583): S1(2,1:2) at xi face points (local faces 2,
+        // 4), S2(1,1:2) at eta face points (1, 3)
+        met2.assign((size_t)NC * 4 * N * 2, 0.0);
+        for (size_t c = 0; c < (size_t)NC; c++)
+            for (int lf = 1; lf <= 4; lf++)
+                for (int nfp = 1; nfp <= N; nfp++) {
+                    int ifp, jfp;  // face2fpconnec, initsetup.f90:347-383
+                    switch (lf) {
+                    case 1: ifp = nfp; jfp = 1; break;
+                    case 2: ifp = N1; jfp = nfp; break;
+                    case 3: ifp = N - nfp + 1; jfp = N1; break;
+                    default: ifp = 1; jfp = N - nfp + 1; break;
+                    }
+                    double *o = &met2[((c * 4 + (lf - 1)) * N + (nfp - 1)) * 2];
+                    if (lf % 2 == 0) {
+                        const size_t b = 4 * ((ifp - 1) + (size_t)N1 * ((jfp - 1) + (size_t)N * c));
+                        o[0] = S1[b + 1];
+                        o[1] = S1[b + 3];
+                    } else {
+                        const size_t b = 4 * ((ifp - 1) + (size_t)N * ((jfp - 1) + (size_t)N1 * c));
+                        o[0] = S2[b + 0];
+                        o[1] = S2[b + 2];
+                    }
+                }
+        CK(cudaMemcpyAsync(ctx->met2, met2.data(), met2.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    }
     CK(cudaMemcpyAsync(ctx->met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->faces, fr.data(), fr.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -409,9 +449,39 @@ StageArgs sddc::base_args(sddc_ctx *ctx)
     return a;
 }
 
+// the viscous chain of the stage input (two launches); the stage kernel then
+// adds its dFv + dGv
+static cudaError_t launch_visc(sddc_ctx *ctx, const double *q_in, const void *t_in)
+{
+    ViscArgs v{};
+    v.ncell = ctx->ncell;
+    v.vismode = ctx->p.vismode;
+    v.mu = ctx->p.mu;
+    v.eta0 = ctx->p.eta0;
+    v.fs = Freestream{ctx->p.rinf, ctx->p.pinf, ctx->p.uinf, ctx->p.vinf, ctx->p.bxinf, ctx->p.byinf};
+    v.q = q_in;
+    v.t_in = t_in;
+    v.met = ctx->met;
+    v.met2 = ctx->met2;
+    v.faces = ctx->faces;
+    v.grad = ctx->visc_grad;
+    v.gt = ctx->visc_gt;
+    v.rv = ctx->visc_rv;
+    switch (ctx->p.precision) {
+    case SDDC_FP64_EXACT: return launch_visc_exact(ctx->N, v, ctx->ops, ctx->stream);
+    case SDDC_FP64: return launch_visc_fp64(ctx->N, v, ctx->ops, ctx->stream);
+    default: return launch_visc_mixed(ctx->N, v, ctx->ops, ctx->stream);
+    }
+}
+
 static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a_in)
 {
     StageArgs a = a_in;
+    if (ctx->visc) {
+        cudaError_t e = launch_visc(ctx, a.q_in, a.t_in);
+        if (e != cudaSuccess) return e;
+        a.visc = ctx->visc_rv;
+    }
     if (ctx->ncase) {  // a batch: one CTA per tile of the case-aligned tile table
         a.tiles = diag ? ctx->tiles_diag : ctx->tiles_rk;
         a.ntiles = diag ? ctx->ntiles_diag : ctx->ntiles_rk;
@@ -678,6 +748,7 @@ static int build_tiles(sddc_ctx *ctx, int cpb, int4 **dev, int *count)
 
 extern "C" int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases)
 {
+    if (ctx && ctx->visc) return set_err(ctx, SDDC_EINVAL, "batches run the ideal chain only (mu = eta0 = 0)");
     if (!ctx || ncase < 1 || !cases) return set_err(ctx, SDDC_EINVAL, "sddc_set_cases: bad arguments");
     // the cases must tile the cell range in order
     int next = 0;

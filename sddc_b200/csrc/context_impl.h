@@ -21,6 +21,10 @@ cudaError_t launch_stage_mixed(int N, int cpb, bool diag, const StageArgs &a, co
 cudaError_t launch_trace_exact(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
 cudaError_t launch_trace_fp64(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
 cudaError_t launch_trace_mixed(int N, int ncell, const double *q, void *t, const Ops &ops, cudaStream_t st);
+struct ViscArgs;
+cudaError_t launch_visc_exact(int N, const ViscArgs &a, const Ops &ops, cudaStream_t st);
+cudaError_t launch_visc_fp64(int N, const ViscArgs &a, const Ops &ops, cudaStream_t st);
+cudaError_t launch_visc_mixed(int N, const ViscArgs &a, const Ops &ops, cudaStream_t st);
 }  // namespace sddc
 
 
@@ -79,6 +83,12 @@ struct sddc_ctx {
     int ntiles_rk = 0, ntiles_diag = 0;
     // discrete adjoint work space (adjoint.cu), created on first use
     sddc::AdjWs *adj = nullptr;
+    // viscous / resistive chain (vismode = 1 with mu or eta0 nonzero)
+    bool visc = false;
+    double *visc_grad = nullptr;  // nablaQs (9,2,N,N,NCELL)
+    double *visc_gt = nullptr;    // gradient traces [cell][lf][nfp][18]
+    double *visc_rv = nullptr;    // dFv + dGv (9,N,N,NCELL)
+    double *met2 = nullptr;       // [cell][lf][nfp][2]: the other normal row at each face point
 };
 
 

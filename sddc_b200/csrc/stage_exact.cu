@@ -4,4 +4,5 @@
 #define SDDC_EXACT_FORM true
 #define SDDC_LAUNCH launch_stage_exact
 #define SDDC_TRACE launch_trace_exact
+#define SDDC_VISC launch_visc_exact
 #include "stage_launch.inc"

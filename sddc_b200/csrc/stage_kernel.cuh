@@ -103,6 +103,7 @@ struct StageArgs {
     double *__restrict__ grad_out;     // (9,2,N,N,NCELL), residual evaluation only
     double *__restrict__ mon_part;     // per-CTA (sum resid^2, sum divB^2), or null
     double *__restrict__ cta_max;      // per-CTA (max eigv, max umax) of this stage, or null
+    const double *__restrict__ visc;   // dFv + dGv (9,N,N,NCELL) of the viscous chain, or null (mu = eta0 = 0)
     unsigned *err_flags;
 };
 
@@ -460,8 +461,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         for (int k = 0; k < 9; k++) {
             const R dF = Fx[i * 9 + k], dG = Fy[j * 9 + k];
             res[k] = (double)(-(dF + dG));
-            // the viscous chain adds exactly +0.0 when mu == eta0 == 0
-            if (a.vismode == 1) res[k] = res[k] + 0.0;
+            // the viscous chain (compresid.f90:34-49); it adds exactly +0.0
+            // when mu == eta0 == 0
+            if (a.vismode == 1) res[k] = res[k] + (a.visc ? a.visc[(size_t)cell * NQ + 9 * (i + N * j) + k] : 0.0);
         }
         // compresid.f90:53-78: 1/Jac, Powell 8-wave and GLM sources
         const double *q = sQ + c * NQ + 9 * (i + N * j);

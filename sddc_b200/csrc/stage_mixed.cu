@@ -4,4 +4,5 @@
 #define SDDC_EXACT_FORM false
 #define SDDC_LAUNCH launch_stage_mixed
 #define SDDC_TRACE launch_trace_mixed
+#define SDDC_VISC launch_visc_mixed
 #include "stage_launch.inc"
