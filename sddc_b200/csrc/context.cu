@@ -167,7 +167,7 @@ static void free_all(sddc_ctx *ctx)
     void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
                     ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags,
                     ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag, ctx->visc_grad, ctx->visc_gt,
-                    ctx->visc_rv, ctx->met2};
+                    ctx->visc_rv, ctx->met2, ctx->max_scratch};
     for (void *b : bufs) cudaFree(b);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     adjoint_free(ctx);
@@ -542,6 +542,7 @@ extern "C" int sddc_compresid(sddc_ctx *ctx)
     a.mon_part = ctx->mon_part;
     CK(launch(ctx, true, a));
     ctx->slot = a.slot_w;
+    ctx->sensor_stale = false;
     ctx->mon_nblk = ctx->ncase ? ctx->ntiles_diag : (ctx->ncell + 7) / 8;
     CK(cudaStreamSynchronize(ctx->stream));
     return check_flags(ctx);
@@ -575,6 +576,8 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
         st[3] = {kRkTwoReg, 3, 4, 0, -1, -1, -1, 5, {F43, F41, F42}, 1u};
         st[4] = {kRkFive, 4, 0, 0, 2, 3, 5, -1, {F56, F51, F52, F53, F54, F55}, 1u | 32u};
     }
+    a.artiv = 0;  // the sensor is evaluated on request (sensor_stale)
+    ctx->last_in = st[4].in;
     for (int k = 0; k < 5; k++) {
         a.rk_kind = st[k].kind;
         a.q_in = P[st[k].in];
@@ -646,16 +649,44 @@ static int run_steps(sddc_ctx *ctx, double dt, int nsteps)
             if (e != cudaSuccess) return cuda_err(ctx, e, "stage launch");
         }
         ctx->ctime += dt;  // ctime = ctime0 + dt after the last stage (iterations.f90:211)
+        ctx->sensor_stale = true;
         ctx->mon_nblk = ctx->ncase ? ctx->ntiles_rk : ctx->grid;
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return check_flags(ctx);
 }
 
+// the AV sensor of the last stage's input (see sensor_stale): a residual
+// evaluation of that register that keeps only the sensor, with the maxima
+// the stage read, on a copy of the running maxima
+static int refresh_sensor(sddc_ctx *ctx)
+{
+    const size_t nmax = (size_t)kSlots * 2 * std::max(ctx->ncase, 1);
+    if (!ctx->max_scratch) {
+        int rc = alloc(ctx, (void **)&ctx->max_scratch, nmax * sizeof(double), "maxima copy");
+        if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->max_scratch, ctx->maxima, nmax * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    StageArgs a = base_args(ctx);
+    a.rk_kind = kRkNone;
+    a.maxima = ctx->max_scratch;
+    a.q_in = ctx->reg[ctx->last_in];
+    a.t_in = ctx->trace[ctx->last_in];
+    a.slot_r = (ctx->slot + kSlots - 1) % kSlots;  // the slot the last stage read
+    a.slot_w = ctx->slot;
+    CK(launch(ctx, true, a));
+    ctx->sensor_stale = false;
+    return SDDC_OK;
+}
+
 extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *nablaQs, double *muAV,
                               double *sm_ind)
 {
     if (!ctx) return SDDC_EINVAL;
+    if ((muAV || sm_ind) && ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
+        int rc = refresh_sensor(ctx);
+        if (rc) return rc;
+    }
     if (Q) CK(cudaMemcpyAsync(Q, ctx->reg[0], ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if ((resid || nablaQs) && !ctx->resid)
         return set_err(ctx, SDDC_ESTATE, "no residual kept: call sddc_compresid first");

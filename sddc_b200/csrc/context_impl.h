@@ -69,6 +69,14 @@ struct sddc_ctx {
     double *host_small = nullptr;  // pinned scratch for small read-backs
     Ops ops{};
     int slot = 0;  // slot holding the running maxima after the last evaluation
+    // The AV sensor enters no residual (its coefficients are zero,
+    // getrusanov.f90:326,328), so the RK stages skip it; when muAV or SM_IND
+    // is read after steps, it is evaluated from the last stage's input
+    // register with the maxima that stage read, which is what the reference
+    // holds after RK_S5P3 / FiveStageRk.
+    bool sensor_stale = false;
+    int last_in = 0;            // register that was the last stage's input
+    double *max_scratch = nullptr;  // copy of the maxima for that evaluation
     int mon_nblk = 0;  // CTAs of the last launch that wrote monitor partials
     bool tables = false, state = false;
     bool traces_stale = true;  // trace[0] does not match reg[0] yet

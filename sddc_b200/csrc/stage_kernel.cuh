@@ -99,8 +99,8 @@ struct StageArgs {
     const int2 *__restrict__ faces;    // (cell, local face) records
     double *maxima;                    // [5][2]: running max of eigv, umax
     double *__restrict__ sm_ind;       // (2,NCELL) AV sensor
-    double *__restrict__ resid_out;    // (9,N,N,NCELL), residual evaluation only
-    double *__restrict__ grad_out;     // (9,2,N,N,NCELL), residual evaluation only
+    double *__restrict__ resid_out;    // (9,N,N,NCELL), residual evaluation only (null: not kept)
+    double *__restrict__ grad_out;     // (9,2,N,N,NCELL), residual evaluation only (null: not kept)
     double *__restrict__ mon_part;     // per-CTA (sum resid^2, sum divB^2), or null
     double *__restrict__ cta_max;      // per-CTA (max eigv, max umax) of this stage, or null
     const double *__restrict__ visc;   // dFv + dGv (9,N,N,NCELL) of the viscous chain, or null (mu = eta0 = 0)
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         // with vismode == 0 the reference never fills nablaQs; its divB
         // source then reads the zeros of the fresh allocation
         if constexpr (DIAG) {
-            if (a.vismode != 1) {
+            if (a.vismode != 1 && a.grad_out) {
                 double *go = a.grad_out + (size_t)cell * (18 * NN) + 18 * (i + N * j);
                 for (int k = 0; k < 18; k++) go[k] = 0.0;
             }
@@ -444,9 +444,11 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             if (var == 5) { gB[0][0] = gx; gB[0][1] = gy; }
             if (var == 6) { gB[1][0] = gx; gB[1][1] = gy; }
             if constexpr (DIAG) {
-                double *go = a.grad_out + (size_t)cell * (18 * NN) + 18 * (i + N * j);
-                go[g] = gx;
-                go[9 + g] = gy;
+                if (a.grad_out) {
+                    double *go = a.grad_out + (size_t)cell * (18 * NN) + 18 * (i + N * j);
+                    go[g] = gx;
+                    go[9 + g] = gy;
+                }
             }
         }
         const double divB = gB[0][0] + gB[1][1];
@@ -592,7 +594,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         const size_t g0 = (size_t)c0 * NQ;
         const int n = ncl * NQ;
         if constexpr (DIAG) {
-            for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sRes[e];
+            if (a.resid_out)
+                for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sRes[e];
         } else {
             double cf[6];
 #pragma unroll

@@ -143,3 +143,27 @@ def test_numerical_fault_reported_not_raised_on_device():
     # the context stays usable
     s.set_state(case_cylinder()[3])
     s.rk_s5p3(1e-3, 1)
+
+
+@pytest.mark.parametrize("name", [n for n in SMALL if n != "wallbox_vis0"])
+@pytest.mark.parametrize("k_stage", [3, 5])
+def test_sensor_after_rk_steps(name, k_stage):
+    """The RK stages skip the AV sensor (it enters no residual); read after
+    steps, muAV and SM_IND are those of the last stage's evaluation, as the
+    reference holds them after RK_S5P3 / FiveStageRk."""
+    m, t, ph, Q, o, s = _pair(name, k_stage=k_stage)
+    dt = 0.5 * cases.cfl_dt(m, Q, t.N)
+    if k_stage == 3:
+        o.rk_s5p3(dt, 3)
+    else:
+        o.five_stage_rk(dt, 3)
+    s.rk_s5p3(dt, 3)
+    a, g = o.state(), s.state(muAV=True, sm_ind=True)
+    assert np.array_equal(g["Q"], a["Q"])
+    _sensor_close(g["sm_ind"], a["sm_ind"])
+    _sensor_close(g["muAV"], a["muAV"])
+    # reading it does not disturb the run
+    o.rk_s5p3(dt, 1) if k_stage == 3 else o.five_stage_rk(dt, 1)
+    s.rk_s5p3(dt, 1)
+    assert np.array_equal(s.state()["Q"], o.state()["Q"])
+    assert s.maxima()["eigvmax"] == o.maxima()["eigvmax"]
