@@ -244,16 +244,33 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         sOpHL[k] = ops.HL[k];
     }
     {
+        // batches of kU independent loads per thread before their stores, so
+        // that each thread keeps several loads in flight
+        constexpr int kU = 4;
         const double *src = a.q_in + (size_t)c0 * NQ;
         const int n = ncl * NQ;
-        for (int k = tid; k < n; k += NT) sQ[k] = __ldg(src + k);
+        for (int k0 = tid; k0 < n; k0 += kU * NT) {
+            double v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < n ? __ldg(src + k0 + u * NT) : 0.0;
+#pragma unroll
+            for (int u = 0; u < kU; u++)
+                if (k0 + u * NT < n) sQ[k0 + u * NT] = v[u];
+        }
         const double *msrc = a.met + (size_t)c0 * ML::kSize;
         const int nm = ncl * ML::kSize;
-        for (int k = tid; k < nm; k += NT) {
-            const int c = k / ML::kSize, o = k - c * ML::kSize;
-            const double v = __ldg(msrc + k);
-            if (o < NM) sNrm[c * NM + o] = (R)v;  // rounded once to the arithmetic type
-            else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
+        for (int k0 = tid; k0 < nm; k0 += kU * NT) {
+            double v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < nm ? __ldg(msrc + k0 + u * NT) : 0.0;
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int k = k0 + u * NT;
+                if (k >= nm) break;
+                const int c = k / ML::kSize, o = k - c * ML::kSize;
+                if (o < NM) sNrm[c * NM + o] = (R)v[u];  // rounded once to the arithmetic type
+                else if (o < NM + NN) sJac[c * NN + (o - NM)] = v[u];
+            }
         }
     }
     const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
@@ -603,25 +620,43 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 const double dt = a.cases ? a.cases[cs].dt : a.dt;
                 cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
             }
-            for (int e = tid; e < n; e += NT) {
-                const size_t g = g0 + e;
-                const double q = sQ[e], r = sRes[e];
-                double o;
-                switch (a.rk_kind) {
-                case kRkAxpy: o = q + cf[0] * r; break;
-                case kRkTwoReg: o = (cf[1] * a.reg_a[g] + cf[2] * q) + cf[0] * r; break;
-                case kRkTwoRegT: o = (cf[1] * a.reg_a[g] + cf[2] * q) + (cf[0] * r) * cf[3]; break;
-                default:
-                    o = ((((cf[1] * a.reg_a[g] + cf[2] * a.reg_b[g]) + cf[3] * a.reg_c[g]) + cf[4] * q) +
-                         cf[5] * a.reg_d[g]) + cf[0] * r;
-                    break;
+            // the register reads of kU elements are issued before their use
+            constexpr int kU = 4;
+            const int kind = a.rk_kind;
+            for (int e0 = tid; e0 < n; e0 += kU * NT) {
+                double ra[kU], rb[kU], rc[kU], rd[kU];
+#pragma unroll
+                for (int u = 0; u < kU; u++) {
+                    const int e = e0 + u * NT;
+                    const size_t g = g0 + (e < n ? e : 0);
+                    ra[u] = kind != kRkAxpy ? a.reg_a[g] : 0.0;
+                    rb[u] = kind == kRkFive ? a.reg_b[g] : 0.0;
+                    rc[u] = kind == kRkFive ? a.reg_c[g] : 0.0;
+                    rd[u] = kind == kRkFive ? a.reg_d[g] : 0.0;
                 }
-                a.q_out[g] = o;
-                if (a.resid_w) a.resid_w[g] = r;
-                sQ[e] = o;  // the sensor read sQ before the barrier above
-                // the float form keeps the output in its arithmetic type for
-                // phase F (the flux buffer is free by now)
-                if constexpr (sizeof(R) != sizeof(double)) reinterpret_cast<R *>(sF)[e] = (R)o;
+#pragma unroll
+                for (int u = 0; u < kU; u++) {
+                    const int e = e0 + u * NT;
+                    if (e >= n) break;
+                    const size_t g = g0 + e;
+                    const double q = sQ[e], r = sRes[e];
+                    double o;
+                    switch (kind) {
+                    case kRkAxpy: o = q + cf[0] * r; break;
+                    case kRkTwoReg: o = (cf[1] * ra[u] + cf[2] * q) + cf[0] * r; break;
+                    case kRkTwoRegT: o = (cf[1] * ra[u] + cf[2] * q) + (cf[0] * r) * cf[3]; break;
+                    default:
+                        o = ((((cf[1] * ra[u] + cf[2] * rb[u]) + cf[3] * rc[u]) + cf[4] * q) + cf[5] * rd[u]) +
+                            cf[0] * r;
+                        break;
+                    }
+                    a.q_out[g] = o;
+                    if (a.resid_w) a.resid_w[g] = r;
+                    sQ[e] = o;  // the sensor read sQ before the barrier above
+                    // the float form keeps the output in its arithmetic type for
+                    // phase F (the flux buffer is free by now)
+                    if constexpr (sizeof(R) != sizeof(double)) reinterpret_cast<R *>(sF)[e] = (R)o;
+                }
             }
         }
     }
