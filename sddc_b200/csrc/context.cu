@@ -515,6 +515,7 @@ int sddc::check_flags(sddc_ctx *ctx)
         std::string m = "device numerics:";
         if (f & kErrNonPositiveDensity) m += " non-positive density";
         if (f & kErrNonFiniteWaveSpeed) m += " non-finite wave speed";
+        if (f & kErrStagingTimeout) m += " staging copy timed out";
         return set_err(ctx, SDDC_ENUMERIC, m);
     }
     return SDDC_OK;

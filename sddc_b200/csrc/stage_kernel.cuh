@@ -117,7 +117,47 @@ template <int N> struct MetLayout {
 };
 
 // error flag bits
-enum : unsigned { kErrNonPositiveDensity = 1u, kErrNonFiniteWaveSpeed = 2u };
+enum : unsigned { kErrNonPositiveDensity = 1u, kErrNonFiniteWaveSpeed = 2u, kErrStagingTimeout = 16u };
+
+// ---- one-dimensional TMA bulk copies into shared memory, completed on an
+// mbarrier (PTX mbarrier.*, cp.async.bulk) -------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// dst and src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait (each try_wait may suspend the thread briefly); false if it
+// gave up
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 22); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
 
 template <int N, typename R, bool DIAG> struct Smem {
     static constexpr int NQ = 9 * N * N;
@@ -235,6 +275,25 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *maxima = a.maxima + 10 * cs;
 
     // ---- stage the state, the metrics and the operators ------------------------
+    // The tile's state slice goes to sQ and its metric records to the flux
+    // buffer (free until phase A) by two TMA bulk copies that one thread
+    // issues, when the slice is 16-byte aligned; otherwise by batches of loads.
+    __shared__ __align__(8) unsigned long long sBar;
+    __shared__ int sAbort;
+    double *sMetRaw = reinterpret_cast<double *>(sF);
+    const size_t qbytes = (size_t)ncl * NQ * sizeof(double);
+    const size_t mbytes = (size_t)ncl * ML::kSize * sizeof(double);
+    const double *qsrc = a.q_in + (size_t)c0 * NQ, *msrc0 = a.met + (size_t)c0 * ML::kSize;
+    const bool bulk = (((uintptr_t)qsrc | (uintptr_t)msrc0 | qbytes | mbytes) & 15) == 0;  // uniform in the CTA
+    if (tid == 0) {
+        sAbort = 0;
+        if (bulk) {
+            mbar_init(&sBar, 1);
+            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes));
+            bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
+            bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
+        }
+    }
     for (int k = tid; k < NP * N; k += NT) {
         sOpL[k] = opL<R>(ops, k);
         sOpM[k] = opM<R>(ops, k);
@@ -243,7 +302,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         sOpH[k] = ops.H[k];
         sOpHL[k] = ops.HL[k];
     }
-    {
+    if (!bulk) {
         // batches of kU independent loads per thread before their stores, so
         // that each thread keeps several loads in flight
         constexpr int kU = 4;
@@ -264,18 +323,29 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < nm ? __ldg(msrc + k0 + u * NT) : 0.0;
 #pragma unroll
-            for (int u = 0; u < kU; u++) {
-                const int k = k0 + u * NT;
-                if (k >= nm) break;
-                const int c = k / ML::kSize, o = k - c * ML::kSize;
-                if (o < NM) sNrm[c * NM + o] = (R)v[u];  // rounded once to the arithmetic type
-                else if (o < NM + NN) sJac[c * NN + (o - NM)] = v[u];
-            }
+            for (int u = 0; u < kU; u++)
+                if (k0 + u * NT < nm) sMetRaw[k0 + u * NT] = v[u];
         }
     }
     const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
     const R c_h = (R)sqrt(eig_r * (eig_r - um_r));
+    if (bulk && tid == 0 && !mbar_wait_bounded(&sBar, 0)) {
+        // the copies did not complete: flag it, give them time to land in
+        // this CTA's shared memory, and leave (every thread, below)
+        atomicOr(a.err_flags, kErrStagingTimeout);
+        sAbort = 1;
+        mbar_wait_bounded(&sBar, 0);
+    }
+    __syncthreads();
+    if (sAbort) return;
+    // the metric record: normals (rounded once to the arithmetic type) and Jac
+    for (int k = tid; k < ncl * ML::kSize; k += NT) {
+        const int c = k / ML::kSize, o = k - c * ML::kSize;
+        const double v = sMetRaw[k];
+        if (o < NM) sNrm[c * NM + o] = (R)v;
+        else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
+    }
     __syncthreads();
 
     // ---- A: interpolate every line to its flux points ---------------------------
