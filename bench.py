@@ -476,8 +476,12 @@ def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
     ph = cases.cylinder_physics(ms=MS, ma=MA)
     Q0 = cases.freestream_state(ph, 4, m.ncell, noise=1e-6, seed=seed)
     dt = cases.cfl_dt(m, Q0, 4)
+    from sddc_b200 import autotune
+
+    cpb, _ = autotune.tune(t, ph, Q0, dt, "fp64_exact", steps=2)
     free0 = torch.cuda.mem_get_info()[0]
-    prob = adjoint.DragLiftProblem(t, dt, nsteps, n1, n2, w_drag=1.0, w_lift=0.0, checkpoint_every=20)
+    prob = adjoint.DragLiftProblem(t, dt, nsteps, n1, n2, w_drag=1.0, w_lift=0.0, checkpoint_every=20,
+                                   cells_per_cta=cpb)
     fs0 = np.array([ph.rinf, ph.pinf, ph.uinf, ph.vinf, ph.bxinf, ph.byinf])
     s = prob.solver(fs0)
     ctx_bytes = free0 - torch.cuda.mem_get_info()[0]
@@ -517,6 +521,7 @@ def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
     stats = r["stats"]
     return {"workload": "cylinder O-grid 128x256, p=3 (N=4), exact FP64 RK_S5P3, "
                         f"{nsteps} steps, J = mean C_D over steps {n1}..{n2}, checkpoints every 20 steps",
+            "cells_per_cta": cpb,
             "J": J, "cd": r["cd"], "cl": r["cl"], "dJ_dMs": dms, "dJ_dMA": dma,
             "dJ_dQ0_l2": float(np.linalg.norm(qbar)),
             "forward_ms": fwd_ms, "recording_forward_ms": stats["forward_ms"], "reverse_ms": stats["reverse_ms"],

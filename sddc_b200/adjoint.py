@@ -59,12 +59,14 @@ class DragLiftProblem:
     stream is a creation parameter of the drop-in)."""
 
     def __init__(self, tables, dt: float, nsteps: int, n1: int, n2: int, w_drag: float = 1.0, w_lift: float = 0.0,
-                 diameter: float = 1.0, checkpoint_every: int = 20, vismode: int = 1, artiv: int = 1):
+                 diameter: float = 1.0, checkpoint_every: int = 20, vismode: int = 1, artiv: int = 1,
+                 cells_per_cta: int = 0):
         self.tables = tables
         self.dt, self.nsteps, self.n1, self.n2 = float(dt), int(nsteps), int(n1), int(n2)
         self.w_drag, self.w_lift, self.diameter = float(w_drag), float(w_lift), float(diameter)
         self.checkpoint_every = int(checkpoint_every)
         self.vismode, self.artiv = vismode, artiv
+        self.cells_per_cta = int(cells_per_cta)
         self._solvers = {}
         self.last = None
 
@@ -73,7 +75,7 @@ class DragLiftProblem:
         s = self._solvers.get(key)
         if s is None:
             ph = cases.Physics(**dict(zip(FREESTREAM, key)), vismode=self.vismode, artiv=self.artiv)
-            s = Solver(self.tables, ph, precision="fp64_exact")
+            s = Solver(self.tables, ph, precision="fp64_exact", cells_per_cta=self.cells_per_cta)
             self._solvers[key] = s
         return s
 

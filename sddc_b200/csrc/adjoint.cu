@@ -222,6 +222,7 @@ int reverse_stage(sddc_ctx *ctx, const RevStage &s)
     a.sy = s.sy;
     for (int i = 0; i < kMaxN; i++) a.wq[i] = w->wq[i];
     a.part = w->part;
+    a.err = ctx->err_flags;
     CKA(launch_vjp(ctx, a));
     const bool own_eig = s.reduce && s.Lnext > s.L, own_um = s.reduce && s.Unext > s.U;
     if (own_eig || own_um) {  // record where the stage raised a running maximum

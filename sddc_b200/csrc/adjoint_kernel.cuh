@@ -73,6 +73,7 @@ struct VjpArgs {
     double sx, sy;
     double wq[kMaxN];
     double *part;  // [8][CTAs]: cbar, pbar[6], 0
+    unsigned *err;
 };
 
 constexpr int kAdjCpb = 4;
@@ -100,31 +101,56 @@ __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, 
 {
     using ML = MetLayout<N>;
     constexpr int NQ = 9 * N * N, NN = N * N, CPB = kTraceCpb;
-    __shared__ double sMu[CPB * NQ];  // -lambda/J
-    __shared__ double sB[CPB * NN];   // Jac, then the divB adjoint over Jac
+    __shared__ __align__(16) double sMu[CPB * NQ];  // lambda source, then -lambda/J
+    __shared__ __align__(16) double sQs[CPB * NQ];  // the state
+    __shared__ double sB[CPB * NN];                 // Jac, then the divB adjoint over Jac
+    __shared__ __align__(8) unsigned long long sBar;
+    __shared__ int sAbort;
     const int tid = threadIdx.x, c0 = blockIdx.x * CPB, ncl = min(CPB, ncell - c0);
+    // the lambda source and state slices by TMA bulk copies when aligned
+    const double *xsrc = xbar + (size_t)c0 * NQ, *qsrc = q + (size_t)c0 * NQ;
+    const size_t bytes = (size_t)ncl * NQ * sizeof(double);
+    const bool bulk = (((uintptr_t)xsrc | (uintptr_t)qsrc | bytes) & 15) == 0;
+    if (tid == 0) {
+        sAbort = 0;
+        if (bulk) {
+            mbar_init(&sBar, 1);
+            mbar_expect_tx(&sBar, (unsigned)(2 * bytes));
+            bulk_g2s(sMu, xsrc, (unsigned)bytes, &sBar);
+            bulk_g2s(sQs, qsrc, (unsigned)bytes, &sBar);
+        }
+    }
     for (int k = tid; k < ncl * NN; k += 128) {
         const int c = k / NN;
         sB[k] = met[(size_t)(c0 + c) * ML::kSize + ML::kJac + (k - c * NN)];
     }
+    if (!bulk)
+        for (int k = tid; k < ncl * NQ; k += 128) {
+            sMu[k] = xsrc[k];
+            sQs[k] = qsrc[k];
+        }
+    if (bulk && tid == 0 && !mbar_wait_bounded(&sBar, 0)) {
+        sAbort = 1;  // the copies did not complete; the caller sees stale traces
+        mbar_wait_bounded(&sBar, 0);
+    }
     __syncthreads();
+    if (sAbort) return;
     // per solution point: the divB adjoint from the Powell source
     // (compresid.f90:60-76), over Jac
     double beta[(CPB * NN + 127) / 128];
     for (int k = tid, it = 0; k < ncl * NN; k += 128, it++) {
-        const size_t g = (size_t)c0 * NQ + 9 * (size_t)k;
-        const double *x = xbar + g;
+        const double *x = sMu + 9 * k;
         double db = 0.0;
         if (vismode == 1) {
-            const double *qq = q + g;
+            const double *qq = sQs + 9 * k;
             const double ux = qq[1] / qq[0], uy = qq[2] / qq[0], uz = qq[3] / qq[0];
             db = -lam_scale * (x[1] * qq[5] + x[2] * qq[6] + x[3] * qq[7] +
                                x[4] * ((ux * qq[5] + uy * qq[6]) + uz * qq[7]) + x[5] * ux + x[6] * uy + x[7] * uz);
         }
         beta[it] = db / sB[k];
     }
-    for (int k = tid; k < ncl * NQ; k += 128)
-        sMu[k] = -(lam_scale * xbar[(size_t)c0 * NQ + k]) / sB[k / 9];
+    __syncthreads();
+    for (int k = tid; k < ncl * NQ; k += 128) sMu[k] = -(lam_scale * sMu[k]) / sB[k / 9];
     __syncthreads();
     for (int k = tid, it = 0; k < ncl * NN; k += 128, it++) sB[k] = beta[it];
     __syncthreads();
@@ -211,7 +237,7 @@ static __device__ __noinline__ void adj_record_face(RecSink rs, Freestream fs, i
 
 // ---- the stage VJP -------------------------------------------------------------
 template <int N, int CPB>
-__global__ void __launch_bounds__(adj_threads(N, CPB), 3) vjp_kernel(const VjpArgs a, const Ops ops)
+__global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpArgs a, const Ops ops)
 {
     using ML = MetLayout<N>;
     constexpr int NT = adj_threads(N, CPB);
@@ -236,23 +262,51 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 3) vjp_kernel(const VjpAr
     const int c0 = blockIdx.x * CPB;
     const int ncl = min(CPB, a.ncell - c0);
 
-    for (int k = tid; k < NP * N; k += NT) {
-        sL[k] = ops.L[k];
-        sM[k] = ops.M[k];
-    }
+    // the tile's state, lambda source and metric slices by TMA bulk copies
+    // (the metric records land in sQf, free until the primal phase) when
+    // they are 16-byte aligned, else by loads
+    __shared__ __align__(8) unsigned long long sBar;
+    __shared__ int sAbort;
     {
-        const double *src = a.q + (size_t)c0 * NQ;
-        for (int k = tid; k < ncl * NQ; k += NT) {
-            sQ[k] = __ldg(src + k);
-            sA[k] = a.xbar ? a.lam_scale * a.xbar[(size_t)c0 * NQ + k] : 0.0;
+        const double *qsrc = a.q + (size_t)c0 * NQ, *msrc = a.met + (size_t)c0 * ML::kSize;
+        const double *xsrc = a.xbar ? a.xbar + (size_t)c0 * NQ : nullptr;
+        const size_t qbytes = (size_t)ncl * NQ * sizeof(double), mbytes = (size_t)ncl * ML::kSize * sizeof(double);
+        const bool bulk = (((uintptr_t)qsrc | (uintptr_t)msrc | (uintptr_t)xsrc | qbytes | mbytes) & 15) == 0;
+        if (tid == 0) {
+            sAbort = 0;
+            if (bulk) {
+                mbar_init(&sBar, 1);
+                mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + (xsrc ? qbytes : 0)));
+                bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
+                bulk_g2s(sQf, msrc, (unsigned)mbytes, &sBar);
+                if (xsrc) bulk_g2s(sA, xsrc, (unsigned)qbytes, &sBar);
+            }
         }
-        const double *msrc = a.met + (size_t)c0 * ML::kSize;
-        for (int k = tid; k < ncl * ML::kSize; k += NT) {
-            const int c = k / ML::kSize, o = k - c * ML::kSize;
-            const double v = __ldg(msrc + k);
-            if (o < NM) sNrm[c * NM + o] = v;
-            else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
+        for (int k = tid; k < NP * N; k += NT) {
+            sL[k] = ops.L[k];
+            sM[k] = ops.M[k];
         }
+        if (!bulk) {
+            for (int k = tid; k < ncl * NQ; k += NT) {
+                sQ[k] = __ldg(qsrc + k);
+                if (xsrc) sA[k] = xsrc[k];
+            }
+            for (int k = tid; k < ncl * ML::kSize; k += NT) sQf[k] = __ldg(msrc + k);
+        }
+        if (bulk && tid == 0 && !mbar_wait_bounded(&sBar, 0)) {
+            atomicOr(a.err, kErrStagingTimeout);  // the copies did not complete
+            sAbort = 1;
+            mbar_wait_bounded(&sBar, 0);
+        }
+    }
+    __syncthreads();
+    if (sAbort) return;
+    for (int k = tid; k < ncl * NQ; k += NT) sA[k] = a.xbar ? a.lam_scale * sA[k] : 0.0;
+    for (int k = tid; k < ncl * ML::kSize; k += NT) {
+        const int c = k / ML::kSize, o = k - c * ML::kSize;
+        const double v = sQf[k];
+        if (o < NM) sNrm[c * NM + o] = v;
+        else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
     }
     __syncthreads();
 
@@ -469,28 +523,23 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 3) vjp_kernel(const VjpAr
                 }
             }
             const double *ql = own_right ? oth : own, *qr = own_right ? own : oth;
-            double qown[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, eig, um, d[9];
+            // this cell's share of the c_h adjoint: its own flux slot
+            cbar += (own_right ? (double)(sign_l * sign_r) : 1.0) * rusanov_wdfdc(ql, qr, n0, n1, sign_l, fown);
+            double qown[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, eig, um;
             // the face-averaged Bx, By feed the gradients of both cells
             qown[5] = 0.5 * vbx;
             qown[6] = 0.5 * vby;
             if (pair) {
                 rusanov_vjp(ql, qr, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, own_right ? nullptr : qown,
-                            own_right ? qown : nullptr, eig, um, d);
+                            own_right ? qown : nullptr, eig, um);
             } else {
                 double qgb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                 qgb[5] = 0.5 * vbx;
                 qgb[6] = 0.5 * vby;
-                rusanov_vjp(own, oth, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, qown, qgb, eig, um, d);
+                rusanov_vjp(own, oth, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, qown, qgb, eig, um);
                 bc_ghost_vjp(kind, own, n0, n1, a.vismode, a.fs, qgb, qown, pb);
             }
-            // this cell's share of the c_h adjoint: its own flux slot
-            {
-                const double m = own_right ? (double)(sign_l * sign_r) : 1.0;
-                double sm = 0.0;
-#pragma unroll
-                for (int k = 0; k < 9; k++) sm += fown[k] * d[k];
-                cbar += m * sm;
-            }
+
 #pragma unroll
             for (int k = 0; k < 9; k++) fown[k] = qown[k];
         }

@@ -263,6 +263,17 @@ SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n
     }
 }
 
+// w . d f / d c_h of the Rusanov flux (f's c_h terms: k = 4, 5, 6, 8)
+SDDC_HD double rusanov_wdfdc(const double *Ql, const double *Qr, double n0, double n1, int sign_l, const double *w)
+{
+    const double magnorm = Sqrt(n0 * n0 + n1 * n1);
+    const double sm = (double)sign_l / magnorm;
+    const double ux = n0 * sm, uy = n1 * sm;
+    const double Bnl = Ql[5] * ux + Ql[6] * uy, Bnr = Qr[5] * ux + Qr[6] * uy;
+    const double K = 0.5 * magnorm * (double)sign_l;
+    return K * (w[4] * (Ql[8] * Bnl + Qr[8] * Bnr) + (w[5] * ux + w[6] * uy) * (Ql[8] + Qr[8]) + w[8] * (Bnl + Bnr));
+}
+
 // d (n0 F_k + n1 G_k) / d c_h at an interior flux point
 SDDC_HD void iflux_dfdc(const double *Q, double n0, double n1, double *d)
 {

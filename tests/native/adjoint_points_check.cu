@@ -112,7 +112,13 @@ int main()
             cc.d[0] = 1.0;
             D1 um3(0.0);
             rusanov<D1, true>(Ql, Qr, Fl, Fr, D1(n0), D1(n1), sl, sr, cc, eig, um3);
-            for (int k = 0; k < 9; k++) report("rusanov dfdc", Fl[k].d[0], dfdc[k], std::fabs(Fl[k].d[0]) + 1.0);
+            double wd = 0.0, ws = 0.0;
+            for (int k = 0; k < 9; k++) {
+                report("rusanov dfdc", Fl[k].d[0], dfdc[k], std::fabs(Fl[k].d[0]) + 1.0);
+                wd += fb[k] * Fl[k].d[0];
+                ws += std::fabs(fb[k] * Fl[k].d[0]);
+            }
+            report("rusanov w.dfdc", wd, rusanov_wdfdc(ql, qr, n0, n1, sl, fb), ws + 1.0);
         }
         // ---- boundary ghost states --------------------------------------------
         {
