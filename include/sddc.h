@@ -39,6 +39,7 @@ extern "C" {
 #define SDDC_ESTATE (-3)      /* call out of order (e.g. no tables yet)       */
 #define SDDC_ENUMERIC (-4)    /* non-positive density or non-finite wave speed seen on the device */
 #define SDDC_ENOMEM (-5)      /* device allocation failed                     */
+#define SDDC_EIO (-6)         /* an output file could not be written          */
 
 /* arithmetic forms of the residual */
 #define SDDC_FP64_EXACT 0  /* the reference's FP64 operations, no FMA: bit-exact to the CPU oracle */
@@ -132,6 +133,45 @@ int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev);
 /* The CUDA stream (cudaStream_t) every launch of the context goes to; for
    callers that order their own work or CUDA events against the drop-in. */
 int sddc_get_stream(sddc_ctx *ctx, void **stream);
+
+/* ---- output from the device state ------------------------------------------
+   The restart and Tecplot files the reference writes every nwrite
+   iterations (iterations.f90:77-80), from the state on the device.  A write
+   call snapshots what it needs on the context's stream and returns; a side
+   stream copies the snapshot to pinned host memory and a host thread writes
+   the file while later calls step on.  A second write of the same kind waits
+   until the first file is written.  sddc_output_wait blocks until every
+   queued file is written and returns the first failure since the last wait
+   (SDDC_EIO with the message in sddc_last_error); sddc_destroy writes what
+   is queued before it returns. */
+
+/* The plot mesh of tecplotter2dsetup (tecplotter2dsetup.f90:1-160), as the
+   host library's sddc_plotmesh_tables gives it: plotx (2,plotnodes),
+   gnumnode (nre+1,nre+1,NCELL), gnode_factor (plotnodes), connec
+   (4,plotcells) with plotcells = nre^2 * NCELL, all 1-based.  Copied. */
+int sddc_set_plot(sddc_ctx *ctx, int nre, int plotnodes, int plotcells, const double *plotx,
+                  const int *gnumnode, const int *gnode_factor, const int *connec);
+
+/* tecplotter2d (tecplotter.f90:1-95) of the current state, synchronous:
+   plotq (9,plotnodes) rho u v w p Bx By Bz psi, plotav (2,plotnodes) muAV
+   and etaAV averaged over the cells at each node (0 unless vismode = 1 and
+   ARTIV = 1: the reference allocates muAV only then, initsetup.f90:36-41).
+   The exact FP64 operations of the reference in its order, for every form.
+   Either pointer may be NULL.  Not for batches. */
+int sddc_plot_nodes(sddc_ctx *ctx, double *plotq, double *plotav);
+
+/* The Tecplot file of tecplotter2d + tecpost_parallel (tecplotter.f90:1-415)
+   for the current state and solution time, written in the background.
+   path NULL: the reference's name, ./TEC/TEC<int(ctime):7><.fff>.plt. */
+int sddc_write_tecplot(sddc_ctx *ctx, const char *path);
+
+/* The restart file of WRITE_ALL_DATA_PARALLEL (write_data.f90:1-83) for the
+   current state and solution time, written in the background.  icg (NCELL)
+   the global cell numbers IC2ICG, NULL for 1..NCELL.  path NULL: the
+   reference's name, restart.<iter:8>.dat in the working directory. */
+int sddc_write_restart(sddc_ctx *ctx, const char *path, int iter, const int *icg);
+
+int sddc_output_wait(sddc_ctx *ctx);
 
 /* ---- batches of independent cases ----------------------------------------
    No counterpart in the reference (its runs are one case each).  Several

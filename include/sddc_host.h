@@ -78,6 +78,53 @@ int sddc_mesh_tables(const sddc_mesh *m, int *if2c, int *if2v, int *ibfinter,
 int sddc_mesh_metrics(const sddc_mesh *m, int N, double *S1, double *S2,
                       double *Jac, double *xxsolu);
 
+/* ---- output (iterations.f90:77-80) ---------------------------------------- */
+
+typedef struct sddc_plotmesh sddc_plotmesh;
+
+/* Plot mesh of the Tecplot output: tecplotter2dsetup
+   (tecplotter2dsetup.f90:1-160) with bilinear cells.  Every cell is split
+   into nre x nre plot cells; plot nodes 1..NVERT are the mesh vertices,
+   then each face's nre-1 inner nodes (made by the first cell that visits
+   the face, matched by position within 1e-5 by the second) and each cell's
+   (nre-1)^2 interior nodes, in the reference's order.  Fails if a vertex
+   is used by no cell or a face node finds no match. */
+int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre);
+void sddc_plotmesh_destroy(sddc_plotmesh *pm);
+int sddc_plotmesh_counts(const sddc_plotmesh *pm, int *plotnodes,
+                         int *plotcells);
+/* plotX(2,plotnodes), gnumnode(nre+1,nre+1,NCELL), gnode_factor(plotnodes),
+   connec_c2n(4,plotcells), all 1-based as the reference holds them; any
+   pointer may be NULL. */
+int sddc_plotmesh_tables(const sddc_plotmesh *pm, double *plotx,
+                         int *gnumnode, int *gnode_factor, int *connec);
+
+/* The reference's file names: 'restart.<iter, 8 digits>.dat'
+   (write_data.f90:45) and 'TEC<int(ctime), 7 digits><.fff>.plt'
+   (tecplotter.f90:176-177).  Return the length, or -1 if buf is short. */
+int sddc_restart_filename(int iter, char *buf, int len);
+int sddc_tecplot_filename(double ctime, char *buf, int len);
+
+/* Restart file of WRITE_ALL_DATA_PARALLEL (write_data.f90:1-83):
+   Q (9,N,N,NCELL); icg (NCELL) the global cell numbers, NULL for 1..NCELL. */
+int sddc_restart_write(const char *path, int iter, double ctime, int N,
+                       int ncell, const int *icg, const double *Q);
+/* READ_ALL_DATA_BINARY (read_data_restart.f90:36-70): reads nrec records
+   (NCELLGLOB; 0 means ncell) and stores each whose global number maps to a
+   local cell: icg2ic (nglob entries, ICG2IC) or, when NULL, the identity. */
+int sddc_restart_read(const char *path, int N, int ncell, int nrec,
+                      const int *icg2ic, int nglob, double *Q, int *iter,
+                      double *ctime);
+
+/* Tecplot file of tecpost_parallel (tecplotter.f90:99-415) from host
+   arrays: plotx (2,plotnodes), plotq (9,plotnodes) as tecplotter2d leaves
+   it (rho u v w p Bx By Bz psi), plotav (2,plotnodes) or NULL for zeros,
+   connec (4,plotcells) 1-based. */
+int sddc_tecplot_write(const char *path, double ctime, int plotnodes,
+                       int plotcells, const double *plotx,
+                       const double *plotq, const double *plotav,
+                       const int *connec);
+
 const char *sddc_host_last_error(void);
 
 #ifdef __cplusplus

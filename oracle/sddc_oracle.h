@@ -111,6 +111,21 @@ void orc_rk_s5p3_combine(int stage, long n, orc_real dt, orc_real *q,
    [0,1]) and summed.  The maxima are not updated. */
 void orc_wall_force(orc_ctx *c, const double *w, orc_real *fx, orc_real *fy);
 
+/* --- output (sddc_oracle_output.c; plain build only) ------------------- */
+/* tecplotter2dsetup (tecplotter2dsetup.f90:1-160), bilinear cells.  Arrays
+   sized for (nre+1)^2*ncell nodes: plotX (2,.), gnode_factor (.),
+   gnumnode (nre+1,nre+1,ncell), connec_c2n (4,nre^2*ncell).  Returns 0, -1
+   if a vertex is used by no cell, -2 if a face node found no match. */
+int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv,
+                   const double *yv, const int *if2c, int nface, int nre,
+                   int *plotnodes, int *plotcells, double *plotX,
+                   int *gnumnode, int *gnode_factor, int *connec_c2n);
+/* tecplotter2d (tecplotter.f90:1-95): plotQ (9,plotnodes) as rho u v w p
+   Bx By Bz psi, plotAV (2,plotnodes); muAV (2,ncell) or NULL for zeros. */
+void orc_plot_eval(int N, int ncell, const double *Q, const double *muAV,
+                   int nre, int plotnodes, const int *gnumnode,
+                   const int *gnode_factor, double *plotQ, double *plotAV);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,7 +66,9 @@ def _load(path, tangent):
     L.orc_setsandpoints.argtypes = [_I, _PD, _PD]
     L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
     L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
-    if not tangent:  # complex scalars by value have no ctypes type
+    if not tangent:  # complex scalars by value have no ctypes type; output routines: plain build
+        L.orc_plot_setup.argtypes = [_I, _I, _PI, _PD, _PD, _PI, _I, _I, _PI, _PI, _PD, _PI, _PI, _PI]
+        L.orc_plot_eval.argtypes = [_I, _I, _PD, _PD, _I, _I, _PI, _PI, _PD, _PD]
         L.orc_point_iflux.argtypes = [_PD, _D, _PD, _PD, _PD]
         L.orc_point_rusanov.argtypes = [_PD, _PD, _PD, _PD, _PD, _I, _I, _D, _PD, _PD, _PD]
         L.orc_rk_s5p3_combine.argtypes = [_I, _L, _D, _PD, _PD, _PD, _PD]
@@ -245,3 +247,92 @@ def rk_s5p3_combine(stage, dt, q, qk0, qka, r):
                               _p(np.ascontiguousarray(qka, dtype=np.float64)),
                               _p(np.ascontiguousarray(r, dtype=np.float64)))
     return q
+
+
+# ---------------------------------------------------------------- output
+# tecplotter2dsetup / tecplotter2d (sddc_oracle_output.c) and a numpy
+# restatement of the file formats of tecpost_parallel (tecplotter.f90:99-415)
+# and WRITE_ALL_DATA_PARALLEL (write_data.f90:1-83), independent of the
+# product's writers.
+
+def plot_setup(ivcell, xv, yv, if2c, nre):
+    """(plotnodes, plotcells, plotX (2,.), gnumnode, gnode_factor, connec (4,.))."""
+    nc = ivcell.shape[0]
+    cap = (nre + 1) ** 2 * nc
+    iv = np.asfortranarray(ivcell, dtype=np.int32)
+    f2c = np.asfortranarray(if2c, dtype=np.int32)
+    px = np.zeros((2, cap), order="F")
+    gn = np.zeros((nre + 1, nre + 1, nc), np.int32, order="F")
+    gf = np.zeros(cap, np.int32)
+    cn = np.zeros((4, nre * nre * nc), np.int32, order="F")
+    nn, ncl = ctypes.c_int(), ctypes.c_int()
+    rc = lib().orc_plot_setup(nc, len(xv), _p(iv, _PI), _p(np.ascontiguousarray(xv, dtype=np.float64)),
+                              _p(np.ascontiguousarray(yv, dtype=np.float64)), _p(f2c, _PI), f2c.shape[0], nre,
+                              ctypes.byref(nn), ctypes.byref(ncl), _p(px), _p(gn, _PI), _p(gf, _PI), _p(cn, _PI))
+    if rc != 0:
+        raise RuntimeError(f"orc_plot_setup failed ({rc})")
+    n = nn.value
+    return n, ncl.value, np.asfortranarray(px[:, :n]), gn, gf[:n].copy(), cn
+
+
+def plot_eval(N, Q, muAV, nre, plotnodes, gnumnode, gnode_factor):
+    """tecplotter2d: (plotQ (9,plotnodes), plotAV (2,plotnodes))."""
+    nc = Q.shape[3]
+    q = np.asfortranarray(Q, dtype=np.float64)
+    mu = None if muAV is None else np.asfortranarray(muAV, dtype=np.float64)
+    pq = np.zeros((9, plotnodes), order="F")
+    pa = np.zeros((2, plotnodes), order="F")
+    lib().orc_plot_eval(N, nc, _p(q), _p(mu), nre, plotnodes, _p(np.asfortranarray(gnumnode, dtype=np.int32), _PI),
+                        _p(np.ascontiguousarray(gnode_factor, dtype=np.int32), _PI), _p(pq), _p(pa))
+    return pq, pa
+
+
+def _fortran_fixed(x, d):
+    """Digits of Fw.d for 0 <= x < 1 from the exact binary value, ties away from zero."""
+    from fractions import Fraction
+    t = Fraction(x) * 10 ** d
+    fl = t.numerator // t.denominator
+    r = t - fl
+    return fl + (1 if r >= Fraction(1, 2) else 0)
+
+
+def restart_name(it):
+    return f"restart.{it:08d}.dat"
+
+
+def tecplot_name(ctime):
+    ip = int(ctime)
+    d = _fortran_fixed(ctime - ip, 3)
+    return f"TEC{ip:07d}.{d % 1000:03d}.plt"
+
+
+def restart_bytes(it, ctime, Q, icg=None):
+    nv, n, _, nc = Q.shape
+    rec = np.dtype([("icg", "<i4"), ("q", "<f8", (nv * n * n,))])
+    body = np.zeros(nc, dtype=rec)
+    body["icg"] = np.arange(1, nc + 1) if icg is None else icg
+    body["q"] = np.asfortranarray(Q).reshape(nv * n * n, nc, order="F").T
+    return np.int32(it).tobytes() + np.float64(ctime).tobytes() + body.tobytes()
+
+
+def _tec_string(s):
+    return np.array([ord(c) for c in s] + [0], dtype="<i4").tobytes()
+
+
+def tecplot_bytes(ctime, plotx, plotq, plotav, connec):
+    names = ["X", "Y", "RHO", "U", "V", "W", "P", "Bx", "By", "Bz", "Az", "muAV", "etaAV"]
+    nn, ncl = plotx.shape[1], connec.shape[1]
+    av = np.zeros((2, nn)) if plotav is None else plotav
+    vals = [plotx[0], plotx[1]] + [plotq[k] for k in range(9)] + [av[0], av[1]]
+    out = [b"#!TDV111", np.array([1, 0], "<i4").tobytes(), _tec_string("step data"),
+           np.int32(len(names)).tobytes()]
+    out += [_tec_string(n) for n in names]
+    out += [np.float32(299.0).tobytes(), _tec_string("ZONE 001"), np.array([-1, 0], "<i4").tobytes(),
+            np.float64(ctime).tobytes(), np.array([-1, 3, 0, 0, 0, 0, nn, ncl, 0, 0, 0, 0], "<i4").tobytes(),
+            np.float32(357.0).tobytes(), np.float32(299.0).tobytes(),
+            np.array([1] * len(names) + [0, 0, -1], "<i4").tobytes()]
+    mm = np.array([[v.min(), v.max()] for v in vals], dtype="<f8")
+    out.append(mm.tobytes())
+    out += [np.asarray(v, dtype="<f4").tobytes() for v in vals]
+    out.append((np.asfortranarray(connec).T.astype("<i4") - 1).tobytes())
+    return b"".join(out)

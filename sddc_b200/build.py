@@ -35,6 +35,7 @@ CUDA_UNITS = {
     "noalloc.cu": [],
     "adjoint.cu": [],
     "adjoint_exact.cu": ["-fmad=false"],
+    "output.cu": ["-fmad=false"],
 }
 
 

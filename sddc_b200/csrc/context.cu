@@ -157,6 +157,7 @@ extern "C" const char *sddc_last_error(const sddc_ctx *ctx) { return ctx ? ctx->
 
 static void free_all(sddc_ctx *ctx)
 {
+    output_free(ctx);
     for (auto &g : ctx->graph)
         if (g) {
             cudaGraphExecDestroy(g);
@@ -680,11 +681,25 @@ static int refresh_sensor(sddc_ctx *ctx)
     return SDDC_OK;
 }
 
+// muAV (2,NCELL) of the current state into ctx->muav, on the stream
+int sddc::device_muav(sddc_ctx *ctx)
+{
+    if (ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
+        int rc = refresh_sensor(ctx);
+        if (rc) return rc;
+    }
+    const double h = std::sqrt(ctx->p.dxcycl * ctx->p.dycycl / (double)ctx->p.ncellglob);
+    muav_kernel<<<(ctx->ncell + 255) / 256, 256, 0, ctx->stream>>>(ctx->ncell, ctx->N, h, ctx->sm_ind, ctx->maxima,
+                                                                   ctx->slot, ctx->muav);
+    CK(cudaGetLastError());
+    return SDDC_OK;
+}
+
 extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *nablaQs, double *muAV,
                               double *sm_ind)
 {
     if (!ctx) return SDDC_EINVAL;
-    if ((muAV || sm_ind) && ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
+    if (sm_ind && ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
         int rc = refresh_sensor(ctx);
         if (rc) return rc;
     }
@@ -696,10 +711,8 @@ extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *n
         CK(cudaMemcpyAsync(nablaQs, ctx->grad, 2 * ctx->nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (muAV && ctx->ncase) return set_err(ctx, SDDC_ESTATE, "muAV is per case; read sm_ind for a batch");
     if (muAV) {
-        const double h = std::sqrt(ctx->p.dxcycl * ctx->p.dycycl / (double)ctx->p.ncellglob);
-        muav_kernel<<<(ctx->ncell + 255) / 256, 256, 0, ctx->stream>>>(ctx->ncell, ctx->N, h, ctx->sm_ind,
-                                                                       ctx->maxima, ctx->slot, ctx->muav);
-        CK(cudaGetLastError());
+        int rc = device_muav(ctx);
+        if (rc) return rc;
         CK(cudaMemcpyAsync(muAV, ctx->muav, 2 * (size_t)ctx->ncell * sizeof(double), cudaMemcpyDeviceToHost,
                            ctx->stream));
     }

@@ -15,6 +15,7 @@
 
 namespace sddc {
 struct AdjWs;
+struct Output;
 cudaError_t launch_stage_exact(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
 cudaError_t launch_stage_fp64(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
 cudaError_t launch_stage_mixed(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
@@ -97,6 +98,8 @@ struct sddc_ctx {
     double *visc_gt = nullptr;    // gradient traces [cell][lf][nfp][18]
     double *visc_rv = nullptr;    // dFv + dGv (9,N,N,NCELL)
     double *met2 = nullptr;       // [cell][lf][nfp][2]: the other normal row at each face point
+    // restart / Tecplot output (output.cu), created on first use
+    sddc::Output *out = nullptr;
 };
 
 
@@ -109,6 +112,8 @@ SDDC_INTERNAL int check_flags(sddc_ctx *ctx);
 SDDC_INTERNAL int met_size(int N);
 SDDC_INTERNAL StageArgs base_args(sddc_ctx *ctx);
 SDDC_INTERNAL void adjoint_free(sddc_ctx *ctx);
+SDDC_INTERNAL void output_free(sddc_ctx *ctx);
+SDDC_INTERNAL int device_muav(sddc_ctx *ctx);
 }  // namespace sddc
 
 #define CK(call)                                                              \

@@ -7,6 +7,8 @@
 //   MAPCYCLOC      map_cyc_loc.f90:1-42       periodic face pairs
 //   setsandpoints / computeLandM  initsetup.f90:171-344
 //   mapder / calcjacob (bilinear) mapder.f90:1-76, calcjacob.f90:1-132
+//   tecplotter2dsetup            tecplotter2dsetup.f90:1-160  plot mesh
+// and the reference's restart and Tecplot file formats (output_format.h).
 // The face numbering and the choice of left cell (the lower cell index,
 // which visits the face first) follow CONNECTIVITY, because the Rusanov flux
 // is evaluated with the left cell's metric and trace first.
@@ -16,10 +18,12 @@
 
 #include "../../include/sddc_host.h"
 #include "sd_basis.h"
+#include "output_format.h"
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -413,4 +417,220 @@ extern "C" int sddc_mesh_metrics(const sddc_mesh *m, int N, double *S1, double *
                 }
     }
     return 0;
+}
+
+// ---------------------------------------------------------------- plot mesh
+
+struct sddc_plotmesh {
+    int nre = 0, ncell = 0, plotnodes = 0, plotcells = 0;
+    std::vector<double> plotx;  // (2,plotnodes)
+    std::vector<int> gnumnode;  // (nre+1,nre+1,ncell)
+    std::vector<int> gfac;      // (plotnodes)
+    std::vector<int> connec;    // (4,plotcells)
+};
+
+// xyCoor_atGps with the bilinear MapBaseFunc (mapder.f90:79-87, 255-273)
+static void bilinear_point(const double X[4], const double Y[4], double xi, double et, double &px, double &py)
+{
+    const double fn[4] = {(1.0 - xi) * (1.0 - et), (1.0 - et) * xi, xi * et, (1.0 - xi) * et};
+    px = 0.0;
+    py = 0.0;
+    for (int k = 0; k < 4; k++) {
+        px = px + X[k] * fn[k];
+        py = py + Y[k] * fn[k];
+    }
+}
+
+extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre)
+{
+    if (!out) return fail(-1, "sddc_plotmesh_build: out is NULL");
+    *out = nullptr;
+    if (!m) return fail(-1, "sddc_plotmesh_build: NULL mesh");
+    if (nre < 1 || nre > 64) return fail(-1, "sddc_plotmesh_build: nre must be in [1, 64]");
+    const int Np = nre, n1 = nre + 1, nc = m->ncell;
+    const size_t cap = (size_t)n1 * n1 * nc;  // allocate_plot_memory
+    if (cap >= (size_t)1 << 31 || (size_t)m->nvert > cap) return fail(-1, "sddc_plotmesh_build: mesh too large");
+    const double tolplot = 1e-5;
+    auto pm = std::make_unique<sddc_plotmesh>();
+    pm->nre = nre;
+    pm->ncell = nc;
+    std::vector<double> px(2 * cap);
+    std::vector<int> gfac(cap, 0), isfacenod(m->nface + 1, 0), gfacenode((size_t)(Np > 1 ? Np - 1 : 1) * (m->nface + 1));
+    pm->gnumnode.assign(cap, 0);
+    auto gn = [&](int ii, int jj, int c) -> int & {
+        return pm->gnumnode[(ii - 1) + (size_t)n1 * ((jj - 1) + (size_t)n1 * (c - 1))];
+    };
+    int plotnodes = 0, plotcells = 0;
+    // the four vertices of each cell: plot nodes 1..NVERT are the vertices
+    for (int c = 1; c <= nc; c++) {
+        const int v[4] = {m->iv(c, 1), m->iv(c, 2), m->iv(c, 3), m->iv(c, 4)};
+        gn(1, 1, c) = v[0];
+        gn(Np + 1, 1, c) = v[1];
+        gn(Np + 1, Np + 1, c) = v[2];
+        gn(1, Np + 1, c) = v[3];
+        for (int k = 0; k < 4; k++) {
+            const int g = v[k];
+            if (gfac[g - 1] == 0) {
+                plotnodes++;
+                px[2 * (g - 1)] = m->xv[g - 1];
+                px[2 * (g - 1) + 1] = m->yv[g - 1];
+            }
+            gfac[g - 1]++;
+        }
+    }
+    if (plotnodes != m->nvert)
+        return fail(-1, "sddc_plotmesh_build: " + std::to_string(m->nvert - plotnodes) +
+                            " vertices belong to no cell (the plot node numbering needs every vertex)");
+    std::vector<int> connec(4 * (size_t)Np * Np * nc);
+    for (int c = 1; c <= nc; c++) {
+        double X[4], Y[4];
+        for (int k = 1; k <= 4; k++) {
+            X[k - 1] = m->xv[m->iv(c, k) - 1];
+            Y[k - 1] = m->yv[m->iv(c, k) - 1];
+        }
+        // the inner nodes of the four faces, counter-clockwise
+        for (int k = 1; k <= 4; k++) {
+            const int iface = m->ic2f[(c - 1) + (size_t)nc * (k - 1)];
+            for (int en = 1; en <= Np - 1; en++) {
+                int ii = 0, jj = 0;
+                switch (k) {
+                case 1: ii = en + 1; jj = 1; break;
+                case 2: ii = Np + 1; jj = en + 1; break;
+                case 3: ii = Np + 1 - en; jj = Np + 1; break;
+                default: ii = 1; jj = Np + 1 - en; break;
+                }
+                const double xsi = (double)(ii - 1) / (double)Np, eta = (double)(jj - 1) / (double)Np;
+                double rx, ry;
+                bilinear_point(X, Y, xsi, eta, rx, ry);
+                if (isfacenod[iface] == 1) {
+                    bool match = false;
+                    for (int e = 1; e <= Np - 1; e++) {
+                        const int g = gfacenode[(e - 1) + (size_t)(Np - 1) * iface];
+                        const double dx = rx - px[2 * (g - 1)], dy = ry - px[2 * (g - 1) + 1];
+                        if (std::fabs(std::sqrt(dx * dx + dy * dy)) <= tolplot) {
+                            gn(ii, jj, c) = g;
+                            gfac[g - 1]++;
+                            match = true;
+                        }
+                    }
+                    if (!match)
+                        return fail(-1, "sddc_plotmesh_build: face " + std::to_string(iface) + " node of cell " +
+                                            std::to_string(c) + " matches none of the face's plot nodes");
+                } else {
+                    plotnodes++;
+                    px[2 * (plotnodes - 1)] = rx;
+                    px[2 * (plotnodes - 1) + 1] = ry;
+                    gn(ii, jj, c) = plotnodes;
+                    gfacenode[(en - 1) + (size_t)(Np - 1) * iface] = plotnodes;
+                    gfac[plotnodes - 1]++;
+                }
+            }
+            if (isfacenod[iface] == 0) isfacenod[iface] = 1;
+        }
+        // interior nodes
+        for (int ii = 2; ii <= Np; ii++)
+            for (int jj = 2; jj <= Np; jj++) {
+                double rx, ry;
+                bilinear_point(X, Y, (double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx, ry);
+                plotnodes++;
+                px[2 * (plotnodes - 1)] = rx;
+                px[2 * (plotnodes - 1) + 1] = ry;
+                gn(ii, jj, c) = plotnodes;
+                gfac[plotnodes - 1]++;
+            }
+        // plot cells
+        for (int ii = 1; ii <= Np; ii++)
+            for (int jj = 1; jj <= Np; jj++) {
+                int *q = &connec[4 * (size_t)plotcells];
+                q[0] = gn(ii, jj, c);
+                q[1] = gn(ii + 1, jj, c);
+                q[2] = gn(ii + 1, jj + 1, c);
+                q[3] = gn(ii, jj + 1, c);
+                plotcells++;
+            }
+    }
+    pm->plotnodes = plotnodes;
+    pm->plotcells = plotcells;
+    px.resize(2 * (size_t)plotnodes);
+    gfac.resize(plotnodes);
+    pm->plotx = std::move(px);
+    pm->gfac = std::move(gfac);
+    pm->connec = std::move(connec);
+    *out = pm.release();
+    return 0;
+}
+
+extern "C" void sddc_plotmesh_destroy(sddc_plotmesh *pm) { delete pm; }
+
+extern "C" int sddc_plotmesh_counts(const sddc_plotmesh *pm, int *plotnodes, int *plotcells)
+{
+    if (!pm) return fail(-1, "sddc_plotmesh_counts: NULL plot mesh");
+    if (plotnodes) *plotnodes = pm->plotnodes;
+    if (plotcells) *plotcells = pm->plotcells;
+    return 0;
+}
+
+extern "C" int sddc_plotmesh_tables(const sddc_plotmesh *pm, double *plotx, int *gnumnode, int *gnode_factor,
+                                    int *connec)
+{
+    if (!pm) return fail(-1, "sddc_plotmesh_tables: NULL plot mesh");
+    if (plotx) std::memcpy(plotx, pm->plotx.data(), pm->plotx.size() * sizeof(double));
+    copy_list(pm->gnumnode, gnumnode);
+    copy_list(pm->gfac, gnode_factor);
+    copy_list(pm->connec, connec);
+    return 0;
+}
+
+// ---------------------------------------------------------------- output files
+
+static int copy_name(const std::string &s, char *buf, int len)
+{
+    if (!buf || len <= (int)s.size()) return fail(-1, "file name buffer too short");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return (int)s.size();
+}
+
+extern "C" int sddc_restart_filename(int iter, char *buf, int len)
+{
+    return copy_name(sddc::fmt::restart_name(iter), buf, len);
+}
+
+extern "C" int sddc_tecplot_filename(double ctime, char *buf, int len)
+{
+    return copy_name(sddc::fmt::tecplot_name(ctime), buf, len);
+}
+
+extern "C" int sddc_restart_write(const char *path, int iter, double ctime, int N, int ncell, const int *icg,
+                                  const double *Q)
+{
+    if (!path || !Q || N < 2 || N > 6 || ncell < 1) return fail(-1, "sddc_restart_write: bad arguments");
+    std::string err;
+    return sddc::fmt::write_restart(path, iter, ctime, N, ncell, icg, Q, err) ? fail(-1, err) : 0;
+}
+
+extern "C" int sddc_restart_read(const char *path, int N, int ncell, int nrec, const int *icg2ic, int nglob,
+                                 double *Q, int *iter, double *ctime)
+{
+    if (!path || !Q || N < 2 || N > 6 || ncell < 1 || nrec < 0 || (icg2ic && nglob < 1))
+        return fail(-1, "sddc_restart_read: bad arguments");
+    std::string err;
+    return sddc::fmt::read_restart(path, N, ncell, nrec ? nrec : ncell, icg2ic, nglob, Q, iter, ctime, err)
+               ? fail(-1, err)
+               : 0;
+}
+
+extern "C" int sddc_tecplot_write(const char *path, double ctime, int plotnodes, int plotcells, const double *plotx,
+                                  const double *plotq, const double *plotav, const int *connec)
+{
+    if (!path || plotnodes < 1 || plotcells < 1 || !plotx || !plotq || !connec)
+        return fail(-1, "sddc_tecplot_write: bad arguments");
+    std::vector<double> zeros;
+    if (!plotav) zeros.assign(2 * (size_t)plotnodes, 0.0);
+    const double *av = plotav ? plotav : zeros.data();
+    sddc::fmt::PlotVar vars[sddc::fmt::kPlotVars] = {{plotx, 2}, {plotx + 1, 2}};
+    for (int v = 0; v < 9; v++) vars[2 + v] = {plotq + v, 9};
+    vars[11] = {av, 2};
+    vars[12] = {av + 1, 2};
+    std::string err;
+    return sddc::fmt::write_tecplot(path, ctime, plotnodes, plotcells, vars, connec, err) ? fail(-1, err) : 0;
 }

@@ -36,6 +36,16 @@ def _lib():
         lib.sddc_mesh_counts.argtypes = [ctypes.c_void_p, _PI]
         lib.sddc_mesh_tables.argtypes = [ctypes.c_void_p] + [_PI] * 10
         lib.sddc_mesh_metrics.argtypes = [ctypes.c_void_p, _I, _PD, _PD, _PD, _PD]
+        lib.sddc_plotmesh_build.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, _I]
+        lib.sddc_plotmesh_destroy.argtypes = [ctypes.c_void_p]
+        lib.sddc_plotmesh_destroy.restype = None
+        lib.sddc_plotmesh_counts.argtypes = [ctypes.c_void_p, _PI, _PI]
+        lib.sddc_plotmesh_tables.argtypes = [ctypes.c_void_p, _PD, _PI, _PI, _PI]
+        lib.sddc_restart_filename.argtypes = [_I, ctypes.c_char_p, _I]
+        lib.sddc_tecplot_filename.argtypes = [_D, ctypes.c_char_p, _I]
+        lib.sddc_restart_write.argtypes = [ctypes.c_char_p, _I, _D, _I, _I, _PI, _PD]
+        lib.sddc_restart_read.argtypes = [ctypes.c_char_p, _I, _I, _I, _PI, _I, _PD, _PI, _PD]
+        lib.sddc_tecplot_write.argtypes = [ctypes.c_char_p, _D, _I, _I, _PD, _PD, _PD, _PI]
         lib.sddc_host_last_error.restype = ctypes.c_char_p
         lib._sddc_typed = True
     return lib
@@ -101,8 +111,7 @@ class Tables:
                 self.ibfree, len(self.ibfree), self.cyc2fpair, int(self.cyc2fpair.shape[0]))
 
 
-def build_tables(mesh, N: int) -> Tables:
-    lib = _lib()
+def _mesh_handle(lib, mesh) -> ctypes.c_void_p:
     iv = np.asfortranarray(mesh.ivcell.astype(np.int32))
     xv = np.ascontiguousarray(mesh.xv, dtype=np.float64)
     yv = np.ascontiguousarray(mesh.yv, dtype=np.float64)
@@ -112,6 +121,12 @@ def build_tables(mesh, N: int) -> Tables:
     _check(lib.sddc_mesh_build(ctypes.byref(h), mesh.ncell, mesh.nvert, ptr(iv, _I), ptr(xv), ptr(yv),
                                int(bt.shape[0]), ptr(bv, _I), ptr(bt, _I), float(mesh.dxcycl),
                                float(mesh.dycycl)), lib)
+    return h
+
+
+def build_tables(mesh, N: int) -> Tables:
+    lib = _lib()
+    h = _mesh_handle(lib, mesh)
     try:
         c = np.zeros(len(MC_FIELDS), dtype=np.int32)
         _check(lib.sddc_mesh_counts(h, ptr(c, _I)), lib)
@@ -140,3 +155,80 @@ def build_tables(mesh, N: int) -> Tables:
                   IF2V=IF2V, ibfinter=lists["inter"], ibfinl=lists["inl"], ibfout=lists["out"],
                   ibfwal=lists["wal"], ibfsymp=lists["symp"], ibfree=lists["free"], cyc2fpair=cyc,
                   ivcell=ivc, counts=counts, dxcycl=float(mesh.dxcycl), dycycl=float(mesh.dycycl))
+
+
+@dataclasses.dataclass
+class PlotMesh:
+    """The Tecplot plot mesh of tecplotter2dsetup (tecplotter2dsetup.f90:1-160), reference layout."""
+
+    nre: int
+    plotnodes: int
+    plotcells: int
+    plotx: np.ndarray         # (2,plotnodes)
+    gnumnode: np.ndarray      # (nre+1,nre+1,NCELL), 1-based node numbers
+    gnode_factor: np.ndarray  # (plotnodes)
+    connec: np.ndarray        # (4,plotcells), 1-based
+
+
+def plot_mesh(mesh, nre: int) -> PlotMesh:
+    lib = _lib()
+    h = _mesh_handle(lib, mesh)
+    pm = ctypes.c_void_p()
+    try:
+        _check(lib.sddc_plotmesh_build(ctypes.byref(pm), h, int(nre)), lib)
+        nn, nc = _I(), _I()
+        _check(lib.sddc_plotmesh_counts(pm, ctypes.byref(nn), ctypes.byref(nc)), lib)
+        px = np.zeros((2, nn.value), order="F")
+        gn = np.zeros((nre + 1, nre + 1, mesh.ncell), np.int32, order="F")
+        gf = np.zeros(nn.value, np.int32)
+        cn = np.zeros((4, nc.value), np.int32, order="F")
+        _check(lib.sddc_plotmesh_tables(pm, ptr(px), ptr(gn, _I), ptr(gf, _I), ptr(cn, _I)), lib)
+    finally:
+        if pm.value:
+            lib.sddc_plotmesh_destroy(pm)
+        lib.sddc_mesh_destroy(h)
+    return PlotMesh(int(nre), nn.value, nc.value, px, gn, gf, cn)
+
+
+def restart_filename(iter_: int) -> str:
+    lib = _lib()
+    b = ctypes.create_string_buffer(64)
+    _check(0 if lib.sddc_restart_filename(int(iter_), b, 64) >= 0 else -1, lib)
+    return b.value.decode()
+
+
+def tecplot_filename(ctime: float) -> str:
+    lib = _lib()
+    b = ctypes.create_string_buffer(64)
+    _check(0 if lib.sddc_tecplot_filename(float(ctime), b, 64) >= 0 else -1, lib)
+    return b.value.decode()
+
+
+def restart_write(path: str, Q: np.ndarray, iter_: int = 0, ctime: float = 0.0, icg=None) -> None:
+    """WRITE_ALL_DATA_PARALLEL's file from a host Q (9,N,N,NCELL)."""
+    lib = _lib()
+    Q = np.asfortranarray(Q, dtype=np.float64)
+    N, nc = Q.shape[1], Q.shape[3]
+    g = None if icg is None else np.ascontiguousarray(icg, dtype=np.int32)
+    _check(lib.sddc_restart_write(str(path).encode(), int(iter_), float(ctime), N, nc,
+                                  None if g is None else ptr(g, _I), ptr(Q)), lib)
+
+
+def restart_read(path: str, N: int, ncell: int, nrec: int = 0, icg2ic=None):
+    """READ_ALL_DATA_BINARY: returns (Q (9,N,N,NCELL), iter, ctime); cells absent from the file stay 0."""
+    lib = _lib()
+    Q = np.zeros((9, N, N, ncell), order="F")
+    m = None if icg2ic is None else np.ascontiguousarray(icg2ic, dtype=np.int32)
+    it, ct = _I(), _D()
+    _check(lib.sddc_restart_read(str(path).encode(), N, ncell, int(nrec), None if m is None else ptr(m, _I),
+                                 0 if m is None else len(m), ptr(Q), ctypes.byref(it), ctypes.byref(ct)), lib)
+    return Q, it.value, ct.value
+
+
+def tecplot_write(path: str, ctime: float, pm: PlotMesh, plotq: np.ndarray, plotav=None) -> None:
+    """tecpost_parallel's file from host plot-node values (9,plotnodes) and (2,plotnodes)."""
+    lib = _lib()
+    pq = np.asfortranarray(plotq, dtype=np.float64)
+    pa = None if plotav is None else np.asfortranarray(plotav, dtype=np.float64)
+    _check(lib.sddc_tecplot_write(str(path).encode(), float(ctime), pm.plotnodes, pm.plotcells, ptr(pm.plotx),
+                                  ptr(pq), None if pa is None else ptr(pa), ptr(pm.connec, _I)), lib)

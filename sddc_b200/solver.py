@@ -27,12 +27,13 @@ _PD = ctypes.POINTER(ctypes.c_double)
 FP64_EXACT, FP64, MIXED = 0, 1, 2
 PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "mixed": MIXED}
 
-OK, EINVAL, ECUDA, ESTATE, ENUMERIC, ENOMEM = 0, -1, -2, -3, -4, -5
+OK, EINVAL, ECUDA, ESTATE, ENUMERIC, ENOMEM, EIO = 0, -1, -2, -3, -4, -5, -6
 
 EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables", "sddc_set_state",
             "sddc_compresid", "sddc_rk_step", "sddc_get_state", "sddc_monitor", "sddc_get_maxima",
             "sddc_state_device_ptr", "sddc_get_stream", "sddc_set_cases", "sddc_rk_step_cases",
-            "sddc_get_case_maxima", "sddc_vjp_resid", "sddc_adjoint_run")
+            "sddc_get_case_maxima", "sddc_vjp_resid", "sddc_adjoint_run", "sddc_set_plot", "sddc_plot_nodes",
+            "sddc_write_tecplot", "sddc_write_restart", "sddc_output_wait")
 
 
 class Params(ctypes.Structure):
@@ -93,6 +94,11 @@ def lib():
         L.sddc_vjp_resid.argtypes = [ctypes.c_void_p, _PD, _PD, _PD]
         L.sddc_adjoint_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(AdjointOpts), _PD, _PD, _PD,
                                        ctypes.POINTER(AdjointStats)]
+        L.sddc_set_plot.argtypes = [ctypes.c_void_p, _I, _I, _I, _PD, _PI, _PI, _PI]
+        L.sddc_plot_nodes.argtypes = [ctypes.c_void_p, _PD, _PD]
+        L.sddc_write_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.sddc_write_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _I, _PI]
+        L.sddc_output_wait.argtypes = [ctypes.c_void_p]
         L._sddc_typed = True
     return L
 
@@ -264,17 +270,53 @@ class Solver:
         return dict(J=obj[0], cd=obj[1], cl=obj[2], Qbar0=Qbar, parbar=par,
                     stats={f: getattr(st, f) for f, _ in AdjointStats._fields_})
 
+    # -- output from the device state ------------------------------------------
+    def set_plot(self, pm):
+        """The plot mesh of the Tecplot output (host.PlotMesh, tecplotter2dsetup)."""
+        self._plot = pm
+        self._check(self._L.sddc_set_plot(self._h, pm.nre, pm.plotnodes, pm.plotcells, ptr(pm.plotx),
+                                          ptr(pm.gnumnode, _I), ptr(pm.gnode_factor, _I), ptr(pm.connec, _I)))
+
+    def plot_nodes(self):
+        """tecplotter2d on the device: (plotQ (9,plotnodes), plotAV (2,plotnodes))."""
+        n = self._plot.plotnodes
+        pq = np.zeros((9, n), order="F")
+        pa = np.zeros((2, n), order="F")
+        self._check(self._L.sddc_plot_nodes(self._h, ptr(pq), ptr(pa)))
+        return pq, pa
+
+    def write_tecplot(self, path=None):
+        """Queues the Tecplot file of the current state (tecpost_parallel's format)."""
+        self._check(self._L.sddc_write_tecplot(self._h, None if path is None else str(path).encode()))
+
+    def write_restart(self, path=None, iter_=0, icg=None):
+        """Queues the restart file of the current state (WRITE_ALL_DATA_PARALLEL's format)."""
+        g = None if icg is None else np.ascontiguousarray(icg, dtype=np.int32)
+        self._check(self._L.sddc_write_restart(self._h, None if path is None else str(path).encode(), int(iter_),
+                                               ptr(g, _I)))
+
+    def output_wait(self):
+        """Blocks until every queued file is written; raises the first failure."""
+        self._check(self._L.sddc_output_wait(self._h))
+
     # -- the reference's time loop -------------------------------------------
-    def iterations(self, dt, maxiter, resid_out=None, iter0=0, ncellglob=None):
+    def iterations(self, dt, maxiter, resid_out=None, iter0=0, ncellglob=None, nwrite=0, outdir=None):
         """The loop of iterations.f90:19-83 with its residual monitor every
         10 iterations (mod(iter,10)==1); returns the monitor rows
-        (iter, ctime, RESIDNORM, divB)."""
+        (iter, ctime, RESIDNORM, divB).  With nwrite > 0 and an output
+        directory, the Tecplot file (outdir/TEC/, when a plot mesh is set)
+        and the restart file (outdir/) are queued after the iterations with
+        mod(iter,nwrite)==1 and after the last one (iterations.f90:77-80),
+        and written while the loop goes on."""
+        import os
         rows = []
         ncg = ncellglob or self.ncell
         it = iter0
         if resid_out:
             with open(resid_out, "w") as f:
                 f.write(" ITER    ctime     RESIDNORM   divB\n")
+        if nwrite and outdir is not None and getattr(self, "_plot", None) is not None:
+            os.makedirs(os.path.join(outdir, "TEC"), exist_ok=True)
         while True:
             it += 1
             self.rk_s5p3(dt, 1)
@@ -286,6 +328,15 @@ class Solver:
                 if resid_out:
                     with open(resid_out, "a") as f:
                         f.write(f" {it} {rows[-1][1]!r} {rn!r} {db!r}\n")
-            if it >= maxiter:
+            last = it >= maxiter
+            if nwrite and outdir is not None and (it % nwrite == 1 or last):
+                from . import host
+                if getattr(self, "_plot", None) is not None:
+                    ct = self.maxima()["ctime"]
+                    self.write_tecplot(os.path.join(outdir, "TEC", host.tecplot_filename(ct)))
+                self.write_restart(os.path.join(outdir, host.restart_filename(it)), it)
+            if last:
                 break
+        if nwrite and outdir is not None:
+            self.output_wait()
         return rows
