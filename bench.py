@@ -305,6 +305,8 @@ def run_ours(args):
         "ensemble": ensemble_run(torch) if not args.no_ensemble and single else None,
         "adjoint": adjoint_bench(torch, nsteps=args.adjoint_steps, n1=args.adjoint_steps * 5 // 6,
                                  n2=args.adjoint_steps) if args.adjoint_steps and single else None,
+        "output": output_bench(torch, solver_mod, c.mesh, t, ph, Q0, dt, TILES["mixed"]["cells_per_cta"])
+        if single and not args.no_output else None,
     }
     print(json.dumps(line))
     if dist:
@@ -459,6 +461,77 @@ def ensemble_run(torch, ncase=64, steps=20, warmup=3, seed=0):
             "batched_over_sequential": t_seq / t_batch}
 
 
+def output_bench(torch, solver_mod, mesh, t, ph, Q0, dt, cpb, steps=200, nwrite=100, nre=4):
+    """Restart + Tecplot output every nwrite steps (iterations.f90:77-80)
+    while stepping: the stepping stream's time with and without output, the
+    stream time each write call adds (state snapshot, plot-node kernel) and
+    the background writer's wall time for the files."""
+    import shutil
+
+    from sddc_b200 import host
+
+    pm = host.plot_mesh(mesh, nre)
+    out = tempfile.mkdtemp(prefix="sddc_out_")
+    s = solver_mod.Solver(t, ph, precision="mixed", cells_per_cta=cpb)
+    s.set_plot(pm)
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def run(with_output):
+        s.set_state(Q0)
+        s.rk_s5p3(dt, 3)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        call_ms = []
+        e0.record(stream)
+        for it in range(1, steps + 1):
+            s.rk_s5p3(dt, 1)
+            if with_output and (it % nwrite == 1 or it == steps):
+                a, b = ev(), ev()
+                a.record(stream)
+                s.write_restart(os.path.join(out, host.restart_filename(it)), it)
+                s.write_tecplot(os.path.join(out, f"TEC{it:07d}.plt"))
+                b.record(stream)
+                call_ms.append((a, b))
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        w0 = time.perf_counter()
+        s.output_wait()
+        drain = time.perf_counter() - w0
+        return ms, [a.elapsed_time(b) for a, b in call_ms], drain
+
+    # one output first, untimed: the restart snapshot and its pinned buffer
+    # are allocated by the first write
+    s.set_state(Q0)
+    s.write_restart(os.path.join(out, "warm.dat"), 0)
+    s.output_wait()
+    base_ms, _, _ = run(False)
+    t0 = time.perf_counter()
+    out_ms, call_ms, drain_s = run(True)
+    wall = time.perf_counter() - t0
+    # the synchronous alternative: read the state back and write on the host
+    w0 = time.perf_counter()
+    q = s.state()["Q"]
+    host.restart_write(os.path.join(out, "sync.dat"), q, steps, 0.0)
+    sync_restart_s = time.perf_counter() - w0
+    nfiles = len(call_ms)
+    rbytes = os.path.getsize(os.path.join(out, host.restart_filename(steps)))
+    tbytes = os.path.getsize(os.path.join(out, f"TEC{steps:07d}.plt"))
+    s.close()
+    shutil.rmtree(out, ignore_errors=True)
+    return {
+        "workload": f"{steps} mixed RK_S5P3 steps, restart + Tecplot (nre={nre}) after steps 1, 101, .., {steps}",
+        "plotnodes": pm.plotnodes, "plotcells": pm.plotcells,
+        "restart_bytes": rbytes, "tecplot_bytes": tbytes, "outputs": nfiles,
+        "ms_per_step_no_output": base_ms / steps, "ms_per_step_with_output": out_ms / steps,
+        "stream_ms_per_output": statistics.median(call_ms) if call_ms else None,
+        "writer_drain_s_after_last_step": drain_s, "wall_s_with_output": wall,
+        "sync_restart_write_s": sync_restart_s,
+        "note": "write calls queue a snapshot on the stepping stream; the files are written by a host thread",
+    }
+
+
 def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
     """The discrete adjoint on the cylinder 128x256, p = 3 (N = 4): the
     objective is C_D averaged over the states after n1..n2 exact RK_S5P3
@@ -599,6 +672,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-case batched ensemble block")
+    ap.add_argument("--no-output", action="store_true", help="skip the restart / Tecplot output block")
     ap.add_argument("--only", choices=["mixed", "fp64", "fp64_exact"], default=None,
                     help="time one form only (the command used for ncu captures)")
     ap.add_argument("--accuracy-steps", type=int, default=2000,

@@ -8,14 +8,14 @@
 // state, or the plot-node kernel into a plot buffer) and records an event; a
 // side stream copies the snapshot to pinned host memory after that event, and
 // a host thread waits for the copy and writes the file while the next steps
-// run.  Each kind of output has one snapshot and one pinned buffer; a second
+// run.  Each kind of output has one snapshot, one pinned buffer and one writer
+// thread, so a restart and a Tecplot file are written side by side; a second
 // write of the same kind waits (on the host) until the first file is written.
 //
 // This unit is compiled without multiply-add contraction: the plot-node
 // values are the reference's FP64 operations in the reference's order, so
 // they match the CPU restatement bit for bit before the conversion to float.
 #include <condition_variable>
-#include <deque>
 #include <mutex>
 #include <thread>
 
@@ -114,17 +114,18 @@ struct Output {
     // snapshots (device) and their pinned host copies
     double *d_buf[2] = {}, *h_buf[2] = {};
     size_t buf_doubles[2] = {};
-    // background writer
-    std::thread worker;
+    // background writers, one per kind; a kind holds at most one job
+    std::thread worker[2];
     std::mutex mu;
     std::condition_variable cv;
-    std::deque<Job> jobs;
+    Job job[2];
+    bool queued[2] = {false, false};
     bool busy[2] = {false, false};  // the kind's buffers are held by a queued or running job
     bool stop = false;
     int err = 0;
     std::string msg;
 
-    void run();
+    void run(int kind);
     void wait_kind(int kind)
     {
         std::unique_lock<std::mutex> lk(mu);
@@ -147,17 +148,17 @@ struct Output {
     }
 };
 
-void Output::run()
+void Output::run(int kind)
 {
     cudaSetDevice(device);
     for (;;) {
         Job j;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv.wait(lk, [&] { return stop || !jobs.empty(); });
-            if (jobs.empty()) return;
-            j = std::move(jobs.front());
-            jobs.pop_front();
+            cv.wait(lk, [&] { return stop || queued[kind]; });
+            if (!queued[kind]) return;
+            j = std::move(job[kind]);
+            queued[kind] = false;
         }
         int rc = SDDC_OK;
         std::string em;
@@ -198,7 +199,8 @@ void sddc::output_free(sddc_ctx *ctx)
         o->stop = true;
     }
     o->cv.notify_all();
-    if (o->worker.joinable()) o->worker.join();  // writes what is queued first
+    for (auto &w : o->worker)
+        if (w.joinable()) w.join();  // each writes what is queued first
     o->free_plot();
     for (int k = 0; k < 2; k++) {
         cudaFree(o->d_buf[k]);
@@ -224,7 +226,7 @@ static int output_init(sddc_ctx *ctx)
         CK(cudaEventCreateWithFlags(&o->ev_in[k], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&o->ev_out[k], cudaEventDisableTiming));
     }
-    o->worker = std::thread([o] { o->run(); });
+    for (int k = 0; k < 2; k++) o->worker[k] = std::thread([o, k] { o->run(k); });
     return SDDC_OK;
 }
 
@@ -262,7 +264,8 @@ static int output_submit(sddc_ctx *ctx, Output::Job &&job, size_t n)
     {
         std::lock_guard<std::mutex> lk(o->mu);
         o->busy[k] = true;
-        o->jobs.push_back(std::move(job));
+        o->queued[k] = true;
+        o->job[k] = std::move(job);
     }
     o->cv.notify_all();
     return SDDC_OK;
@@ -343,6 +346,8 @@ extern "C" int sddc_set_plot(sddc_ctx *ctx, int nre, int plotnodes, int plotcell
     CK(cudaMemcpyAsync(o->gfac, gnode_factor, (size_t)plotnodes * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(o->hv, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    // the snapshot and pinned buffers now, not in the first write call
+    if ((rc = output_buffers(ctx, kJobTecplot, (size_t)kPlotOut * plotnodes))) return rc;
     o->plotx.assign(plotx, plotx + 2 * (size_t)plotnodes);
     o->connec.assign(connec, connec + 4 * (size_t)plotcells);
     o->nre = nre;
