@@ -78,18 +78,30 @@ int sddc_mesh_tables(const sddc_mesh *m, int *if2c, int *if2v, int *ibfinter,
 int sddc_mesh_metrics(const sddc_mesh *m, int N, double *S1, double *S2,
                       double *Jac, double *xxsolu);
 
+/* calcjacob with 8-node serendipity cells (CURVE_WALL = 1: MAPDER_8_NODE,
+   mapder.f90:117-253; calcjacob.f90:12-132): S1, S2, Jac as
+   sddc_mesh_metrics, from xxf_cell (2,8,NCELL), the eight nodes of each cell
+   as READ_VRT8_DATA reads them (readGRIDinfo.f90:86-117): corners 1-4
+   counter-clockwise, then the mid-side nodes of edges 1-2, 2-3, 3-4, 4-1.
+   xxsolu (2,N,N,NCELL), if not NULL, from the same map (MapBaseFunc8). */
+int sddc_metrics8(int N, int ncell, const double *xxf_cell, double *S1,
+                  double *S2, double *Jac, double *xxsolu);
+
 /* ---- output (iterations.f90:77-80) ---------------------------------------- */
 
 typedef struct sddc_plotmesh sddc_plotmesh;
 
 /* Plot mesh of the Tecplot output: tecplotter2dsetup
-   (tecplotter2dsetup.f90:1-160) with bilinear cells.  Every cell is split
+   (tecplotter2dsetup.f90:1-160).  Every cell is split
    into nre x nre plot cells; plot nodes 1..NVERT are the mesh vertices,
    then each face's nre-1 inner nodes (made by the first cell that visits
    the face, matched by position within 1e-5 by the second) and each cell's
    (nre-1)^2 interior nodes, in the reference's order.  Fails if a vertex
-   is used by no cell or a face node finds no match. */
-int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre);
+   is used by no cell or a face node finds no match.  xxf_cell (2,8,NCELL)
+   places the face and interior nodes by the 8-node map (CURVE_WALL = 1);
+   NULL for bilinear cells. */
+int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre,
+                        const double *xxf_cell);
 void sddc_plotmesh_destroy(sddc_plotmesh *pm);
 int sddc_plotmesh_counts(const sddc_plotmesh *pm, int *plotnodes,
                          int *plotcells);

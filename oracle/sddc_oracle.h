@@ -111,15 +111,25 @@ void orc_rk_s5p3_combine(int stage, long n, orc_real dt, orc_real *q,
    [0,1]) and summed.  The maxima are not updated. */
 void orc_wall_force(orc_ctx *c, const double *w, orc_real *fx, orc_real *fy);
 
+/* --- 8-node cells, CURVE_WALL = 1 (sddc_oracle_curved.c; plain build) - */
+/* MAPDER_8_NODE + calcjacob (mapder.f90:117-253, calcjacob.f90:1-132) from
+   xxf_cell (2,8,NCELL) (readGRIDinfo.f90:86-117) */
+void orc_calcjacob_8node(int N, int ncell, const double *xxf_cell, double *S1,
+                         double *S2, double *Jac);
+/* xyCoor_atGps(8, xxs, xi, eta, xx) with MapBaseFunc8 */
+void orc_xycoor8(const double *xxs, double xi, double eta, double *xx);
+
 /* --- output (sddc_oracle_output.c; plain build only) ------------------- */
-/* tecplotter2dsetup (tecplotter2dsetup.f90:1-160), bilinear cells.  Arrays
+/* tecplotter2dsetup (tecplotter2dsetup.f90:1-160); xxf_cell (2,8,ncell)
+   for 8-node cells (CURVE_WALL = 1), NULL for bilinear ones.  Arrays
    sized for (nre+1)^2*ncell nodes: plotX (2,.), gnode_factor (.),
    gnumnode (nre+1,nre+1,ncell), connec_c2n (4,nre^2*ncell).  Returns 0, -1
    if a vertex is used by no cell, -2 if a face node found no match. */
 int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv,
-                   const double *yv, const int *if2c, int nface, int nre,
-                   int *plotnodes, int *plotcells, double *plotX,
-                   int *gnumnode, int *gnode_factor, int *connec_c2n);
+                   const double *yv, const double *xxf_cell, const int *if2c,
+                   int nface, int nre, int *plotnodes, int *plotcells,
+                   double *plotX, int *gnumnode, int *gnode_factor,
+                   int *connec_c2n);
 /* tecplotter2d (tecplotter.f90:1-95): plotQ (9,plotnodes) as rho u v w p
    Bx By Bz psi, plotAV (2,plotnodes); muAV (2,ncell) or NULL for zeros. */
 void orc_plot_eval(int N, int ncell, const double *Q, const double *muAV,

@@ -67,7 +67,8 @@ def _load(path, tangent):
     L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
     L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
     if not tangent:  # complex scalars by value have no ctypes type; output routines: plain build
-        L.orc_plot_setup.argtypes = [_I, _I, _PI, _PD, _PD, _PI, _I, _I, _PI, _PI, _PD, _PI, _PI, _PI]
+        L.orc_plot_setup.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PI, _I, _I, _PI, _PI, _PD, _PI, _PI, _PI]
+        L.orc_calcjacob_8node.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
         L.orc_plot_eval.argtypes = [_I, _I, _PD, _PD, _I, _I, _PI, _PI, _PD, _PD]
         L.orc_point_iflux.argtypes = [_PD, _D, _PD, _PD, _PD]
         L.orc_point_rusanov.argtypes = [_PD, _PD, _PD, _PD, _PD, _I, _I, _D, _PD, _PD, _PD]
@@ -255,7 +256,18 @@ def rk_s5p3_combine(stage, dt, q, qk0, qka, r):
 # and WRITE_ALL_DATA_PARALLEL (write_data.f90:1-83), independent of the
 # product's writers.
 
-def plot_setup(ivcell, xv, yv, if2c, nre):
+def metrics8(N: int, xxf_cell: np.ndarray):
+    """calcjacob with 8-node cells (CURVE_WALL = 1): (S1, S2, Jac)."""
+    nc = xxf_cell.shape[2]
+    xx = np.asfortranarray(xxf_cell, dtype=np.float64)
+    S1 = np.zeros((2, 2, N + 1, N, nc), order="F")
+    S2 = np.zeros((2, 2, N, N + 1, nc), order="F")
+    J = np.zeros((N, N, nc), order="F")
+    lib().orc_calcjacob_8node(N, nc, _p(xx), _p(S1), _p(S2), _p(J))
+    return S1, S2, J
+
+
+def plot_setup(ivcell, xv, yv, if2c, nre, xxf_cell=None):
     """(plotnodes, plotcells, plotX (2,.), gnumnode, gnode_factor, connec (4,.))."""
     nc = ivcell.shape[0]
     cap = (nre + 1) ** 2 * nc
@@ -266,8 +278,10 @@ def plot_setup(ivcell, xv, yv, if2c, nre):
     gf = np.zeros(cap, np.int32)
     cn = np.zeros((4, nre * nre * nc), np.int32, order="F")
     nn, ncl = ctypes.c_int(), ctypes.c_int()
+    xx = None if xxf_cell is None else np.asfortranarray(xxf_cell, dtype=np.float64)
     rc = lib().orc_plot_setup(nc, len(xv), _p(iv, _PI), _p(np.ascontiguousarray(xv, dtype=np.float64)),
-                              _p(np.ascontiguousarray(yv, dtype=np.float64)), _p(f2c, _PI), f2c.shape[0], nre,
+                              _p(np.ascontiguousarray(yv, dtype=np.float64)), _p(xx), _p(f2c, _PI),
+                              f2c.shape[0], nre,
                               ctypes.byref(nn), ctypes.byref(ncl), _p(px), _p(gn, _PI), _p(gf, _PI), _p(cn, _PI))
     if rc != 0:
         raise RuntimeError(f"orc_plot_setup failed ({rc})")

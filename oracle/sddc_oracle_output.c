@@ -30,8 +30,8 @@ static void xycoor4(const double xxs[2][4], double xi, double eta, double rx[2])
 }
 
 int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv, const double *yv,
-                   const int *if2c, int nface, int nre, int *plotnodes_out, int *plotcells_out,
-                   double *plotX, int *gnumnode, int *gnode_factor, int *connec_c2n)
+                   const double *xxf_cell, const int *if2c, int nface, int nre, int *plotnodes_out,
+                   int *plotcells_out, double *plotX, int *gnumnode, int *gnode_factor, int *connec_c2n)
 {
     const int Np = nre, NCELL = ncell;
     const double tolplot = 1e-5;
@@ -77,6 +77,8 @@ int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv, co
             xxs[0][j - 1] = xv[IVCELL(icell, j) - 1];
             xxs[1][j - 1] = yv[IVCELL(icell, j) - 1];
         }
+        /* CURVE_WALL = 1: xyCoor_atGps(8, xxf_cell(:,:,icell), ...) */
+        const double *xx8 = xxf_cell ? xxf_cell + 16L * (icell - 1) : NULL;
         for (int k = 1; k <= 4; k++) {
             int iface = IC2F(icell, k);
             for (int enode = 1; enode <= Np - 1; enode++) {
@@ -88,7 +90,8 @@ int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv, co
                 default: ii = 1; jj = Np + 1 - enode; break;
                 }
                 double xsi = (double)(ii - 1) / (double)Np, eta = (double)(jj - 1) / (double)Np, rx[2];
-                xycoor4(xxs, xsi, eta, rx);
+                if (xx8) orc_xycoor8(xx8, xsi, eta, rx);
+                else xycoor4(xxs, xsi, eta, rx);
                 if (isfacenod[iface] == 1) {
                     int checkmatch = 0;
                     for (int existnode = 1; existnode <= Np - 1; existnode++) {
@@ -116,7 +119,8 @@ int orc_plot_setup(int ncell, int nvert, const int *ivcell, const double *xv, co
         for (int ii = 2; ii <= Np; ii++)
             for (int jj = 2; jj <= Np; jj++) {
                 double rx[2];
-                xycoor4(xxs, (double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx);
+                if (xx8) orc_xycoor8(xx8, (double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx);
+                else xycoor4(xxs, (double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx);
                 plotnodes = plotnodes + 1;
                 PX(1, plotnodes) = rx[0];
                 PX(2, plotnodes) = rx[1];

@@ -122,4 +122,4 @@ def mach_gradients(problem: DragLiftProblem, ms: float, ma: float, noise=None):
     Q0 = freestream_field(fs, t.N, t.ncell, noise)
     J = DragLift.apply(Q0, fs, problem)
     J.backward()
-    return float(J), float(ms_t.grad), float(ma_t.grad), problem.last["Qbar0"]
+    return float(J.detach()), float(ms_t.grad), float(ma_t.grad), problem.last["Qbar0"]

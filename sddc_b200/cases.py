@@ -118,8 +118,8 @@ class Case:
 
 
 def cylinder_case(nr: int, nt: int, N: int, steps: int = 500, ms: float = 1.5, ma: float = 2.0,
-                  seed: int = 0, noise: float = 1e-6) -> Case:
-    m = meshmod.cylinder_ogrid(nr, nt)
+                  seed: int = 0, noise: float = 1e-6, curved: bool = False) -> Case:
+    m = meshmod.cylinder_ogrid(nr, nt, curved=curved)
     return Case(name=f"cylinder_{nr}x{nt}_p{N - 1}", mesh=m, N=N, physics=cylinder_physics(ms, ma),
                 steps=steps, seed=seed, noise=noise)
 

@@ -7,6 +7,8 @@
 //   MAPCYCLOC      map_cyc_loc.f90:1-42       periodic face pairs
 //   setsandpoints / computeLandM  initsetup.f90:171-344
 //   mapder / calcjacob (bilinear) mapder.f90:1-76, calcjacob.f90:1-132
+//   MAPDER_8_NODE / calcjacob (8-node serendipity cells, CURVE_WALL = 1)
+//                                mapder.f90:88-253, calcjacob.f90:12-132
 //   tecplotter2dsetup            tecplotter2dsetup.f90:1-160  plot mesh
 // and the reference's restart and Tecplot file formats (output_format.h).
 // The face numbering and the choice of left cell (the lower cell index,
@@ -419,6 +421,108 @@ extern "C" int sddc_mesh_metrics(const sddc_mesh *m, int N, double *S1, double *
     return 0;
 }
 
+// ---------------------------------------------------------------- 8-node cells
+
+// derivatives of the eight serendipity shape functions at (psi, eta)
+// (MAPDER_8_NODE, mapder.f90:117-253; nodes 1-4 the corners counter-
+// clockwise, 5-8 the mid-side nodes of edges 1-2, 2-3, 3-4, 4-1)
+static void shape_derivs8(double psi, double eta, double d[8][2])
+{
+    d[0][0] = (1.0 - eta) * (4.0 * psi + 2.0 * eta - 3.0);
+    d[0][1] = (1.0 - psi) * (4.0 * eta + 2.0 * psi - 3.0);
+    d[1][0] = (1.0 - eta) * (4.0 * psi - 2.0 * eta - 1.0);
+    d[1][1] = psi * (4.0 * eta - 2.0 * psi - 1.0);
+    d[2][0] = eta * (4.0 * psi + 2.0 * eta - 3.0);
+    d[2][1] = psi * (4.0 * eta + 2.0 * psi - 3.0);
+    d[3][0] = eta * (4.0 * psi - 2.0 * eta - 1.0);
+    d[3][1] = (1.0 - psi) * (4.0 * eta - 2.0 * psi - 1.0);
+    d[4][0] = 4.0 * (1.0 - eta) * (1.0 - 2.0 * psi);
+    d[4][1] = 4.0 * psi * (psi - 1.0);
+    d[5][0] = 4.0 * eta * (1.0 - eta);
+    d[5][1] = 4.0 * psi * (1.0 - 2.0 * eta);
+    d[6][0] = 4.0 * eta * (1.0 - 2.0 * psi);
+    d[6][1] = 4.0 * psi * (1.0 - psi);
+    d[7][0] = 4.0 * eta * (eta - 1.0);
+    d[7][1] = 4.0 * (1.0 - psi) * (1.0 - 2.0 * eta);
+}
+
+// calcjacob's CURVE_WALL = 1 sums, k = 1..8 in order (calcjacob.f90:47-52)
+static Derivs map_derivs8(const double *xx, double psi, double eta)
+{
+    double d[8][2];
+    shape_derivs8(psi, eta, d);
+    Derivs r{0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < 8; k++) {
+        r.xpsi = r.xpsi + d[k][0] * xx[2 * k];
+        r.ypsi = r.ypsi + d[k][0] * xx[2 * k + 1];
+        r.xeta = r.xeta + d[k][1] * xx[2 * k];
+        r.yeta = r.yeta + d[k][1] * xx[2 * k + 1];
+    }
+    return r;
+}
+
+// xyCoor_atGps with MapBaseFunc8 (mapder.f90:91-103, 255-273)
+static void serendipity_point(const double *xx, double xi, double eta, double &px, double &py)
+{
+    const double f[8] = {(1.0 - xi) * (1.0 - eta) * (-2.0 * xi - 2.0 * eta + 1.0),
+                         xi * (1.0 - eta) * (2.0 * xi - 2.0 * eta - 1.0),
+                         xi * eta * (2.0 * xi + 2.0 * eta - 3.0),
+                         (1.0 - xi) * eta * (-2.0 * xi + 2.0 * eta - 1.0),
+                         4.0 * (1.0 - eta) * (1.0 - xi) * xi,
+                         4.0 * eta * (1.0 - eta) * xi,
+                         4.0 * (1.0 - xi) * xi * eta,
+                         4.0 * (1.0 - eta) * (1.0 - xi) * eta};
+    px = 0.0;
+    py = 0.0;
+    for (int k = 0; k < 8; k++) {
+        px = px + xx[2 * k] * f[k];
+        py = py + xx[2 * k + 1] * f[k];
+    }
+}
+
+extern "C" int sddc_metrics8(int N, int ncell, const double *xxf_cell, double *S1, double *S2, double *Jac,
+                             double *xxsolu)
+{
+    if (N < 2 || N > 6) return fail(-1, "sddc_metrics8: N must be in [2, 6]");
+    if (ncell < 1 || !xxf_cell) return fail(-1, "sddc_metrics8: bad arguments");
+    double Xs[8], Xf[8];
+    sd_points(N, Xs, Xf);
+    const int N1 = N + 1;
+    for (int c = 0; c < ncell; c++) {
+        const double *xx = xxf_cell + 16 * (size_t)c;  // xxf_cell(2,8,NCELL)
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++) {
+                const size_t ip = (i - 1) + (size_t)N * ((j - 1) + (size_t)N * c);
+                if (Jac) {
+                    Derivs d = map_derivs8(xx, Xs[i - 1], Xs[j - 1]);
+                    Jac[ip] = d.xpsi * d.yeta - d.xeta * d.ypsi;
+                }
+                if (xxsolu) serendipity_point(xx, Xs[i - 1], Xs[j - 1], xxsolu[2 * ip], xxsolu[2 * ip + 1]);
+            }
+        if (S1)
+            for (int j = 1; j <= N; j++)
+                for (int f = 1; f <= N1; f++) {
+                    Derivs d = map_derivs8(xx, Xf[f - 1], Xs[j - 1]);
+                    size_t b = 4 * ((f - 1) + (size_t)N1 * ((j - 1) + (size_t)N * c));
+                    S1[b + 0] = d.yeta;
+                    S1[b + 1] = -d.ypsi;
+                    S1[b + 2] = -d.xeta;
+                    S1[b + 3] = d.xpsi;
+                }
+        if (S2)
+            for (int f = 1; f <= N1; f++)
+                for (int i = 1; i <= N; i++) {
+                    Derivs d = map_derivs8(xx, Xs[i - 1], Xf[f - 1]);
+                    size_t b = 4 * ((i - 1) + (size_t)N * ((f - 1) + (size_t)N1 * c));
+                    S2[b + 0] = d.yeta;
+                    S2[b + 1] = -d.ypsi;
+                    S2[b + 2] = -d.xeta;
+                    S2[b + 3] = d.xpsi;
+                }
+    }
+    return 0;
+}
+
 // ---------------------------------------------------------------- plot mesh
 
 struct sddc_plotmesh {
@@ -441,7 +545,7 @@ static void bilinear_point(const double X[4], const double Y[4], double xi, doub
     }
 }
 
-extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre)
+extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int nre, const double *xxf_cell)
 {
     if (!out) return fail(-1, "sddc_plotmesh_build: out is NULL");
     *out = nullptr;
@@ -488,6 +592,12 @@ extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int 
             X[k - 1] = m->xv[m->iv(c, k) - 1];
             Y[k - 1] = m->yv[m->iv(c, k) - 1];
         }
+        // the cell's map: bilinear, or the eight nodes of xxf_cell
+        const double *xx8 = xxf_cell ? xxf_cell + 16 * (size_t)(c - 1) : nullptr;
+        auto point = [&](double xi, double et, double &px_, double &py_) {
+            if (xx8) serendipity_point(xx8, xi, et, px_, py_);
+            else bilinear_point(X, Y, xi, et, px_, py_);
+        };
         // the inner nodes of the four faces, counter-clockwise
         for (int k = 1; k <= 4; k++) {
             const int iface = m->ic2f[(c - 1) + (size_t)nc * (k - 1)];
@@ -501,7 +611,7 @@ extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int 
                 }
                 const double xsi = (double)(ii - 1) / (double)Np, eta = (double)(jj - 1) / (double)Np;
                 double rx, ry;
-                bilinear_point(X, Y, xsi, eta, rx, ry);
+                point(xsi, eta, rx, ry);
                 if (isfacenod[iface] == 1) {
                     bool match = false;
                     for (int e = 1; e <= Np - 1; e++) {
@@ -531,7 +641,7 @@ extern "C" int sddc_plotmesh_build(sddc_plotmesh **out, const sddc_mesh *m, int 
         for (int ii = 2; ii <= Np; ii++)
             for (int jj = 2; jj <= Np; jj++) {
                 double rx, ry;
-                bilinear_point(X, Y, (double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx, ry);
+                point((double)(ii - 1) / (double)Np, (double)(jj - 1) / (double)Np, rx, ry);
                 plotnodes++;
                 px[2 * (plotnodes - 1)] = rx;
                 px[2 * (plotnodes - 1) + 1] = ry;

@@ -36,7 +36,8 @@ def _lib():
         lib.sddc_mesh_counts.argtypes = [ctypes.c_void_p, _PI]
         lib.sddc_mesh_tables.argtypes = [ctypes.c_void_p] + [_PI] * 10
         lib.sddc_mesh_metrics.argtypes = [ctypes.c_void_p, _I, _PD, _PD, _PD, _PD]
-        lib.sddc_plotmesh_build.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, _I]
+        lib.sddc_metrics8.argtypes = [_I, _I, _PD, _PD, _PD, _PD, _PD]
+        lib.sddc_plotmesh_build.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, _I, _PD]
         lib.sddc_plotmesh_destroy.argtypes = [ctypes.c_void_p]
         lib.sddc_plotmesh_destroy.restype = None
         lib.sddc_plotmesh_counts.argtypes = [ctypes.c_void_p, _PI, _PI]
@@ -147,7 +148,11 @@ def build_tables(mesh, N: int) -> Tables:
         S2 = np.zeros((2, 2, N, N + 1, nc), order="F")
         Jac = np.zeros((N, N, nc), order="F")
         xx = np.zeros((2, N, N, nc), order="F")
-        _check(lib.sddc_mesh_metrics(h, N, ptr(S1), ptr(S2), ptr(Jac), ptr(xx)), lib)
+        if mesh.curved:  # CURVE_WALL = 1: the 8-node map
+            x8 = np.asfortranarray(mesh.xxf_cell, dtype=np.float64)
+            _check(lib.sddc_metrics8(N, nc, ptr(x8), ptr(S1), ptr(S2), ptr(Jac), ptr(xx)), lib)
+        else:
+            _check(lib.sddc_mesh_metrics(h, N, ptr(S1), ptr(S2), ptr(Jac), ptr(xx)), lib)
     finally:
         lib.sddc_mesh_destroy(h)
     Xs, Xf, L, M = sd_operators(N)
@@ -175,7 +180,8 @@ def plot_mesh(mesh, nre: int) -> PlotMesh:
     h = _mesh_handle(lib, mesh)
     pm = ctypes.c_void_p()
     try:
-        _check(lib.sddc_plotmesh_build(ctypes.byref(pm), h, int(nre)), lib)
+        x8 = None if not mesh.curved else np.asfortranarray(mesh.xxf_cell, dtype=np.float64)
+        _check(lib.sddc_plotmesh_build(ctypes.byref(pm), h, int(nre), ptr(x8)), lib)
         nn, nc = _I(), _I()
         _check(lib.sddc_plotmesh_counts(pm, ctypes.byref(nn), ctypes.byref(nc)), lib)
         px = np.zeros((2, nn.value), order="F")

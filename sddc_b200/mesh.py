@@ -7,7 +7,10 @@ The reference reads three text files (readGRIDinfo.f90):
 * vertex file, one line per vertex: ``IV X Y`` (READ_VRT_DATA, :40-84);
 * boundary file, one line per boundary face:
   ``IB IV1 IV2 IREGION IPATCH TYPE`` with TYPE one of INLE, OUTL, SYMP, WALL,
-  CYCL, FREE (READ_BND_DATA, :233-290).
+  CYCL, FREE (READ_BND_DATA, :233-290);
+* with CURVE_WALL = 1, the 8-node file: eight lines ``X Y`` per cell in
+  global cell order, corners 1-4 counter-clockwise then the mid-side nodes
+  of edges 1-2, 2-3, 3-4, 4-1 (READ_VRT8_DATA, :86-117).
 
 The reference ships no meshes, so the cases are generated here:
 
@@ -16,7 +19,9 @@ The reference ships no meshes, so the cases are generated here:
   counter-clockwise, the seam sharing its vertices (a rotational seam cannot
   be expressed as a translation-only CYCL pair, connect_bdry.f90:281-298).
   The inner ring is WALL; the outer ring is INLE where the free stream enters
-  (u_inf . n < 0) and OUTL elsewhere.
+  (u_inf . n < 0) and OUTL elsewhere.  ``curved=True`` adds the 8-node cells
+  whose circumferential edges are circular arcs (their mid-side nodes on the
+  circle), the reference's CURVE_WALL = 1 geometry.
 * ``periodic_box``: a uniform box with every outer face CYCL.
 * ``channel_box``: a box with one boundary type per side and optionally
   perturbed interior vertices (curved metrics), to exercise every BCFLUX
@@ -50,6 +55,11 @@ class Mesh:
     dxcycl: float = 1.0
     dycycl: float = 1.0
     name: str = "mesh"
+    xxf_cell: np.ndarray | None = None  # (2,8,NCELL) Fortran order: 8-node cells (CURVE_WALL = 1)
+
+    @property
+    def curved(self) -> bool:
+        return self.xxf_cell is not None
 
     @property
     def ncell(self) -> int:
@@ -83,10 +93,17 @@ class Mesh:
         with open(paths["bnd"], "w") as f:
             for i, ((a, b), t) in enumerate(zip(self.bnd_v, self.bnd_type), 1):
                 f.write(f"{i} {a} {b} 1 1 {BC_NAMES[t]}\n")
+        if self.curved:
+            paths["vrt8"] = os.path.join(directory, f"{stem}.vrt8")
+            with open(paths["vrt8"], "w") as f:
+                for c in range(nc):
+                    for k in range(8):
+                        f.write(f"{self.xxf_cell[0, k, c]:.17e} {self.xxf_cell[1, k, c]:.17e}\n")
         return paths
 
     @classmethod
-    def read(cls, cel: str, vrt: str, bnd: str, dxcycl: float = 1.0, dycycl: float = 1.0) -> "Mesh":
+    def read(cls, cel: str, vrt: str, bnd: str, dxcycl: float = 1.0, dycycl: float = 1.0,
+             vrt8: str | None = None) -> "Mesh":
         c = np.loadtxt(cel, dtype=np.int64, ndmin=2)
         v = np.loadtxt(vrt, dtype=np.float64, ndmin=2)
         order = np.argsort(v[:, 0])
@@ -99,6 +116,10 @@ class Mesh:
                     continue
                 bv.append((int(parts[1]), int(parts[2])))
                 bt.append(BC_CODE[parts[5][:4].upper()])
+        xx8 = None
+        if vrt8 is not None:
+            a = np.loadtxt(vrt8, dtype=np.float64, ndmin=2)  # (8*NCELL, 2)
+            xx8 = np.asfortranarray(a.reshape(c.shape[0], 8, 2).transpose(2, 1, 0))
         return cls(
             xv=np.ascontiguousarray(v[:, 1]),
             yv=np.ascontiguousarray(v[:, 2]),
@@ -108,7 +129,23 @@ class Mesh:
             dxcycl=dxcycl,
             dycycl=dycycl,
             name=os.path.splitext(os.path.basename(cel))[0],
+            xxf_cell=xx8,
         )
+
+
+def eight_node_cells(m: Mesh, mid=None) -> np.ndarray:
+    """xxf_cell (2,8,NCELL): the corners of each cell and its mid-side nodes.
+    ``mid(xa, ya, xb, yb)`` places the node between two corners (arrays over
+    cells); the default is the straight midpoint, which makes the 8-node map
+    equal the bilinear one."""
+    iv = m.ivcell - 1
+    X, Y = m.xv[iv], m.yv[iv]  # (NCELL, 4)
+    xx = np.zeros((2, 8, m.ncell), order="F")
+    xx[0, :4], xx[1, :4] = X.T, Y.T
+    mid = mid or (lambda xa, ya, xb, yb: (0.5 * (xa + xb), 0.5 * (ya + yb)))
+    for k, (a, b) in enumerate(((0, 1), (1, 2), (2, 3), (3, 0))):
+        xx[0, 4 + k], xx[1, 4 + k] = mid(X[:, a], Y[:, a], X[:, b], Y[:, b])
+    return xx
 
 
 def radial_ratio(nr: int, ratio32: float = 1.08) -> float:
@@ -123,7 +160,7 @@ def radial_ratio(nr: int, ratio32: float = 1.08) -> float:
 
 
 def cylinder_ogrid(nr: int, nt: int, r0: float = 0.5, r1: float = 20.0, ratio: float | None = None,
-                   uinf: float = 1.0, vinf: float = 0.0) -> Mesh:
+                   uinf: float = 1.0, vinf: float = 0.0, curved: bool = False) -> Mesh:
     """O-grid around a cylinder of radius ``r0``; cells ordered ring by ring."""
     q = radial_ratio(nr) if ratio is None else ratio
     if abs(q - 1.0) < 1e-14:
@@ -157,8 +194,21 @@ def cylinder_ogrid(nr: int, nt: int, r0: float = 0.5, r1: float = 20.0, ratio: f
         inflow = uinf * math.cos(tm) + vinf * math.sin(tm) < 0.0
         bv.append((vid(k, nr), vid(k + 1, nr)))
         bt.append(BC_CODE["INLE" if inflow else "OUTL"])
-    return Mesh(xv, yv, ivcell, np.asarray(bv, np.int32), np.asarray(bt, np.int32),
-                name=f"cyl{nr}x{nt}")
+    m = Mesh(xv, yv, ivcell, np.asarray(bv, np.int32), np.asarray(bt, np.int32), name=f"cyl{nr}x{nt}")
+    if curved:
+        def arc_mid(xa, ya, xb, yb):
+            # an edge between two vertices of one ring is the arc between
+            # them; a radial edge is straight
+            ra, rb = np.hypot(xa, ya), np.hypot(xb, yb)
+            same = np.abs(ra - rb) <= 1e-12 * np.maximum(ra, rb)
+            ta, tb = np.arctan2(ya, xa), np.arctan2(yb, xb)
+            dt = np.angle(np.exp(1j * (tb - ta)))  # the short way round, across the seam too
+            tm = ta + 0.5 * dt
+            return (np.where(same, ra * np.cos(tm), 0.5 * (xa + xb)),
+                    np.where(same, ra * np.sin(tm), 0.5 * (ya + yb)))
+        m.xxf_cell = eight_node_cells(m, arc_mid)
+        m.name = f"cyl{nr}x{nt}c"
+    return m
 
 
 def periodic_box(nx: int, ny: int, lx: float = 2.0 * np.pi, ly: float = 2.0 * np.pi) -> Mesh:

@@ -67,6 +67,41 @@ def case_wall_box(nx=4, ny=4, N=4, vismode=1, seed=4):
     return case_channel(nx, ny, N, sides=("WALL", "OUTL", "SYMP", "INLE"), jitter=0.15, vismode=vismode, seed=seed)
 
 
+def wavy_periodic_box(n=6, amp=0.08):
+    """A periodic box of 8-node cells whose edges bulge by a periodic
+    sine (shared and periodic partner edges get the same mid-side node)."""
+    m = mesh.periodic_box(n, n)
+    L = 2 * math.pi
+    h = L / n
+
+    def mid(xa, ya, xb, yb):
+        mx, my = 0.5 * (xa + xb), 0.5 * (ya + yb)
+        d = amp * h * np.sin(2 * math.pi * mx / L) * np.sin(2 * math.pi * my / L)
+        return mx + d, my - d
+
+    m.xxf_cell = mesh.eight_node_cells(m, mid)
+    m.name = f"wavy{n}x{n}"
+    return m
+
+
+def case_cylinder_curved(nr=6, nt=12, N=4, seed=5):
+    """The O-grid with 8-node cells (arcs for the circumferential edges)."""
+    m = mesh.cylinder_ogrid(nr, nt, curved=True)
+    t = host.build_tables(m, N)
+    ph = cases.cylinder_physics(ms=0.5, ma=2.0)
+    Q = cases.freestream_state(ph, N, m.ncell, noise=1e-3, seed=seed)
+    return m, t, ph, Q
+
+
+def case_wavy(n=5, N=5, seed=6):
+    m = wavy_periodic_box(n)
+    t = host.build_tables(m, N)
+    ph = cases.Physics(rinf=1.0, pinf=1.0, uinf=0.3, vinf=-0.2, bxinf=0.4, byinf=0.1, dxcycl=2 * math.pi,
+                       dycycl=2 * math.pi)
+    Q = smooth_state(t, ph, seed=seed)
+    return m, t, ph, Q
+
+
 ALL_SMALL = {
     "cylinder_n4": lambda: case_cylinder(N=4),
     "cylinder_n5": lambda: case_cylinder(N=5),
@@ -76,4 +111,6 @@ ALL_SMALL = {
     "periodic_n4": lambda: case_periodic(N=4),
     "wallbox_vis1": lambda: case_wall_box(vismode=1),
     "wallbox_vis0": lambda: case_wall_box(vismode=0),
+    "cylinder_curved_n4": lambda: case_cylinder_curved(N=4),
+    "wavybox_n5": lambda: case_wavy(N=5),
 }
