@@ -310,6 +310,10 @@ int forward_steps(sddc_ctx *ctx, double dt, int step0, int nsteps, double *const
             a.slot_r = g;
             a.slot_w = g + 1;
             a.cta_max = cmax + (size_t)(5 * m + k) * 2 * fgrid;
+            if (!ctx->nrm_double) {  // the exact kernel reads double normals: convert the packed record
+                a.nrm = nullptr;
+                a.jac = nullptr;
+            }
             CKA(launch_stage_exact(ctx->N, ctx->cpb, false, a, ctx->ops, ctx->stream));
         }
         const int n = step0 + m + 1;

@@ -165,7 +165,7 @@ static void free_all(sddc_ctx *ctx)
         }
     for (auto &r : ctx->reg) cudaFree(r), r = nullptr;
     for (auto &t : ctx->trace) cudaFree(t), t = nullptr;
-    void *bufs[] = {ctx->met, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
+    void *bufs[] = {ctx->met, ctx->nrm, ctx->jac, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
                     ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags,
                     ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag, ctx->visc_grad, ctx->visc_gt,
                     ctx->visc_rv, ctx->met2, ctx->max_scratch};
@@ -231,7 +231,11 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
     const size_t nc = p->ncell;
     const int diag_grid = (p->ncell + 7) / 8;
     const int mon_blocks = std::max(ctx->grid, diag_grid);
+    ctx->nrm_double = p->precision != SDDC_MIXED;
+    const size_t n_nrm = nc * 4 * p->N * (p->N + 1), n_jac = nc * ((p->N * p->N + 1) & ~1);
     if ((rc = alloc(ctx, (void **)&ctx->met, nc * ctx->msize * sizeof(double), "metrics")) ||
+        (rc = alloc(ctx, &ctx->nrm, n_nrm * (ctx->nrm_double ? sizeof(double) : sizeof(float)), "normals")) ||
+        (rc = alloc(ctx, (void **)&ctx->jac, n_jac * sizeof(double), "Jacobians")) ||
         (rc = alloc(ctx, (void **)&ctx->faces, nc * 4 * sizeof(int2), "faces")) ||
         (rc = alloc(ctx, (void **)&ctx->maxima, kSlots * 2 * sizeof(double), "maxima")) ||
         (rc = alloc(ctx, (void **)&ctx->sm_ind, nc * 2 * sizeof(double), "sensor")) ||
@@ -308,6 +312,21 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
                 m[kFam + 2 * (i * N1 + r) + 1] = S2[b + 3];
             }
         for (int k = 0; k < N * N; k++) m[kJac + k] = Jac[k + (size_t)N * N * c];
+    }
+    // the same, split: normals (rounded once to the form's type) and Jac
+    // padded to an even count, so that a tile's slices are 16-byte aligned
+    const int NJ = (N * N + 1) & ~1;
+    std::vector<double> nrm_d, jac((size_t)NC * NJ, 0.0);
+    std::vector<float> nrm_f;
+    if (ctx->nrm_double) nrm_d.resize((size_t)NC * kJac);
+    else nrm_f.resize((size_t)NC * kJac);
+    for (size_t c = 0; c < (size_t)NC; c++) {
+        const double *m = &met[c * ctx->msize];
+        for (int o = 0; o < kJac; o++) {
+            if (ctx->nrm_double) nrm_d[c * kJac + o] = m[o];
+            else nrm_f[c * kJac + o] = (float)m[o];
+        }
+        for (int k = 0; k < N * N; k++) jac[c * NJ + k] = m[kJac + k];
     }
     // per-(cell, local face) records from the reference's face lists
     std::vector<int2> fr((size_t)NC * 4, make_int2(-1, 0));
@@ -388,6 +407,13 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
                            ctx->stream));
     }
     CK(cudaMemcpyAsync(ctx->met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->nrm_double)
+        CK(cudaMemcpyAsync(ctx->nrm, nrm_d.data(), nrm_d.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    else
+        CK(cudaMemcpyAsync(ctx->nrm, nrm_f.data(), nrm_f.size() * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    CK(cudaMemcpyAsync(ctx->jac, jac.data(), jac.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->faces, fr.data(), fr.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->tables = true;
@@ -443,6 +469,8 @@ StageArgs sddc::base_args(sddc_ctx *ctx)
     a.alpha = 2.0;  // initsetup.f90:165
     a.fs = Freestream{ctx->p.rinf, ctx->p.pinf, ctx->p.uinf, ctx->p.vinf, ctx->p.bxinf, ctx->p.byinf};
     a.met = ctx->met;
+    a.nrm = ctx->nrm;
+    a.jac = ctx->jac;
     a.faces = ctx->faces;
     a.maxima = ctx->maxima;
     a.sm_ind = ctx->sm_ind;

@@ -62,6 +62,11 @@ struct sddc_ctx {
     void *trace[sddc::kRegs] = {};  // face traces of each register (float in the mixed form)
     size_t trace_bytes = 0;
     double *met = nullptr;
+    // the metrics split for the stage kernel's staging copies: normals in the
+    // form's arithmetic type [NCELL][4N(N+1)] and Jac [NCELL][kJacPad]
+    void *nrm = nullptr;
+    double *jac = nullptr;
+    bool nrm_double = true;  // normals stored as double (FP64 forms)
     int2 *faces = nullptr;
     double *maxima = nullptr;  // [sddc::kSlots][2]
     double *sm_ind = nullptr, *muav = nullptr, *resid = nullptr, *grad = nullptr;

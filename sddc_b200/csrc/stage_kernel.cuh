@@ -19,9 +19,11 @@
 //      reference scatters to them;
 //   C  divergence of the flux, gradient of (Bx, By) from the face-averaged
 //      flux-point states, Powell and GLM sources (thread per solution point);
-//   D  the AV smoothness sensor per cell;
-//   E  the RK stage update, element-wise over the CTA's contiguous slice of
-//      the state (coalesced loads of the RK registers and stores);
+//   D  the AV smoothness sensor per cell (residual evaluations only);
+//   E  in a time step, the RK stage update of each point by the thread of
+//      phase C: the RK register slice was staged by TMA with the state, the
+//      output is formed in shared memory and stored by one TMA bulk copy
+//      while phase F runs; in a residual evaluation, the residual copy-out;
 //   F  the face traces of the output state, published for the next stage.
 // Running maxima of the wave speed and of the velocity (the c_h input of
 // the next stage) go through atomicMax on five rotating slots, so that
@@ -96,6 +98,11 @@ struct StageArgs {
     const double *reg_d;
     double *resid_w;                   // residual copy (FiveStageRk stage 4 resid0)
     const double *__restrict__ met;    // packed metrics, per cell
+    // the same metrics split for direct staging: normals in the arithmetic
+    // type [NCELL][4N(N+1)] and Jac [NCELL][MetLayout::kJacPad]; null: the
+    // kernel converts the packed record
+    const void *__restrict__ nrm;
+    const double *__restrict__ jac;
     const int2 *__restrict__ faces;    // (cell, local face) records
     double *maxima;                    // [5][2]: running max of eigv, umax
     double *__restrict__ sm_ind;       // (2,NCELL) AV sensor
@@ -112,6 +119,7 @@ template <int N> struct MetLayout {
     static constexpr int kFam = 2 * N * (N + 1);       // doubles per family
     static constexpr int kJac = 2 * kFam;              // offset of Jac(i,j) at kJac + i + N*j
     static constexpr int kSize = (2 * kFam + N * N + 1) & ~1;
+    static constexpr int kJacPad = (N * N + 1) & ~1;  // Jac per cell in the split layout (16-byte rows)
     // normal (S1(1,1:2) or S2(2,1:2)) of family f, line l, flux point r
     __host__ __device__ static constexpr int normal(int f, int l, int r) { return f * kFam + 2 * (l * (N + 1) + r); }
 };
@@ -158,6 +166,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+// shared-memory writes of this thread made visible to the bulk-copy (async)
+// proxy, before a barrier after which one thread issues a bulk store
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// shared -> global bulk store; src and dst 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the issuing thread's bulk stores have read their shared-memory source
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 
 template <int N, typename R, bool DIAG> struct Smem {
     static constexpr int NQ = 9 * N * N;
@@ -209,7 +230,9 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    size_t d = (size_t)CPB * (2 * S::NQ + 2 * N * N + S::kLow) + 4 * 32 + 2 * (N - 1) * N;
+    // sQ, sA, sJac; the sensor's sJz and sLow in residual evaluations only
+    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) + 4 * 32 +
+               2 * (N - 1) * N;
     size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam) + 2 * (N + 1) * N;
     return d * sizeof(double) + r * sizeof(R);
 }
@@ -240,13 +263,15 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NM = 2 * ML::kFam;  // normals per cell
+    constexpr int NJ = ML::kJacPad;
     double *sQ = reinterpret_cast<double *>(smem_raw);          // [CPB][NQ]
-    double *sJac = sQ + CPB * NQ;                                // [CPB][NN]
-    double *sJz = sJac + CPB * NN;                               // [CPB][NN]  Jz^2 for the sensor
-    double *sLow = sJz + CPB * NN;                               // [CPB][kLow]
-    double *sRed = sLow + CPB * S::kLow;                         // [4][32] block reductions
-    double *sRes = sRed + 4 * 32;                                // [CPB][NQ] residual
-    double *sOpH = sRes + CPB * NQ;                              // [N-1][N]  AV projection
+    double *sJac = sQ + CPB * NQ;                                // [CPB][NJ]
+    double *sJz = sJac + CPB * NJ;                               // [CPB][NN]  Jz^2 for the sensor (DIAG)
+    double *sLow = sJz + (DIAG ? CPB * NN : 0);                  // [CPB][kLow] (DIAG)
+    double *sRed = sLow + (DIAG ? CPB * S::kLow : 0);            // [4][32] block reductions
+    // residual (DIAG); in a time step the RK register, then the output
+    double *sA = sRed + 4 * 32;                                  // [CPB][NQ]
+    double *sOpH = sA + CPB * NQ;                                // [N-1][N]  AV projection
     double *sOpHL = sOpH + (N - 1) * N;                          // [N][N-1]  AV prolongation
     R *sNrm = reinterpret_cast<R *>(sOpHL + N * (N - 1));        // [CPB][NM] flux-point normals
     R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
@@ -275,23 +300,43 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *maxima = a.maxima + 10 * cs;
 
     // ---- stage the state, the metrics and the operators ------------------------
-    // The tile's state slice goes to sQ and its metric records to the flux
-    // buffer (free until phase A) by two TMA bulk copies that one thread
-    // issues, when the slice is 16-byte aligned; otherwise by batches of loads.
+    // The tile's state slice goes to sQ, its normals to sNrm and Jac to sJac
+    // (or, without the split metric arrays, its packed metric records to the
+    // flux buffer, free until phase A, for conversion) and, in a stage that
+    // reads one RK register, that register's slice to sA, by TMA bulk copies
+    // that one thread issues when every slice is 16-byte aligned; otherwise
+    // by batches of loads.
     __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sAbort;
     double *sMetRaw = reinterpret_cast<double *>(sF);
+    const bool split = a.nrm != nullptr;  // uniform
+    const bool want_ra = !DIAG && (a.rk_kind == kRkTwoReg || a.rk_kind == kRkTwoRegT);
     const size_t qbytes = (size_t)ncl * NQ * sizeof(double);
-    const size_t mbytes = (size_t)ncl * ML::kSize * sizeof(double);
-    const double *qsrc = a.q_in + (size_t)c0 * NQ, *msrc0 = a.met + (size_t)c0 * ML::kSize;
-    const bool bulk = (((uintptr_t)qsrc | (uintptr_t)msrc0 | qbytes | mbytes) & 15) == 0;  // uniform in the CTA
+    const size_t mbytes = split ? 0 : (size_t)ncl * ML::kSize * sizeof(double);
+    const size_t nbytes = split ? (size_t)ncl * NM * sizeof(R) : 0;
+    const size_t jbytes = split ? (size_t)ncl * NJ * sizeof(double) : 0;
+    const double *qsrc = a.q_in + (size_t)c0 * NQ;
+    const double *msrc0 = a.met + (size_t)c0 * ML::kSize;
+    const R *nsrc = split ? reinterpret_cast<const R *>(a.nrm) + (size_t)c0 * NM : nullptr;
+    const double *jsrc = split ? a.jac + (size_t)c0 * NJ : nullptr;
+    const double *rsrc = want_ra ? a.reg_a + (size_t)c0 * NQ : nullptr;
+    const bool bulk = ((uintptr_t)qsrc & 15) == 0 && (qbytes & 15) == 0 &&
+                      (split ? (((uintptr_t)nsrc | (uintptr_t)jsrc | nbytes | jbytes) & 15) == 0
+                             : (((uintptr_t)msrc0 | mbytes) & 15) == 0) &&
+                      (!want_ra || ((uintptr_t)rsrc & 15) == 0);  // uniform in the CTA
     if (tid == 0) {
         sAbort = 0;
         if (bulk) {
             mbar_init(&sBar, 1);
-            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes));
+            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes + (want_ra ? qbytes : 0)));
             bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
-            bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
+            if (split) {
+                bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
+                bulk_g2s(sJac, jsrc, (unsigned)jbytes, &sBar);
+            } else {
+                bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
+            }
+            if (want_ra) bulk_g2s(sA, rsrc, (unsigned)qbytes, &sBar);
         }
     }
     for (int k = tid; k < NP * N; k += NT) {
@@ -305,27 +350,25 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     if (!bulk) {
         // batches of kU independent loads per thread before their stores, so
         // that each thread keeps several loads in flight
-        constexpr int kU = 4;
-        const double *src = a.q_in + (size_t)c0 * NQ;
-        const int n = ncl * NQ;
-        for (int k0 = tid; k0 < n; k0 += kU * NT) {
-            double v[kU];
+        auto stage_copy = [&](auto *dst, const auto *src, int n) {
+            constexpr int kU = 4;
+            for (int k0 = tid; k0 < n; k0 += kU * NT) {
+                decltype(+src[0]) v[kU];
 #pragma unroll
-            for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < n ? __ldg(src + k0 + u * NT) : 0.0;
+                for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < n ? __ldg(src + k0 + u * NT) : decltype(+src[0])(0);
 #pragma unroll
-            for (int u = 0; u < kU; u++)
-                if (k0 + u * NT < n) sQ[k0 + u * NT] = v[u];
+                for (int u = 0; u < kU; u++)
+                    if (k0 + u * NT < n) dst[k0 + u * NT] = v[u];
+            }
+        };
+        stage_copy(sQ, qsrc, ncl * NQ);
+        if (split) {
+            stage_copy(sNrm, nsrc, ncl * NM);
+            stage_copy(sJac, jsrc, ncl * NJ);
+        } else {
+            stage_copy(sMetRaw, msrc0, ncl * ML::kSize);
         }
-        const double *msrc = a.met + (size_t)c0 * ML::kSize;
-        const int nm = ncl * ML::kSize;
-        for (int k0 = tid; k0 < nm; k0 += kU * NT) {
-            double v[kU];
-#pragma unroll
-            for (int u = 0; u < kU; u++) v[u] = k0 + u * NT < nm ? __ldg(msrc + k0 + u * NT) : 0.0;
-#pragma unroll
-            for (int u = 0; u < kU; u++)
-                if (k0 + u * NT < nm) sMetRaw[k0 + u * NT] = v[u];
-        }
+        if (want_ra) stage_copy(sA, rsrc, ncl * NQ);
     }
     const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
@@ -339,14 +382,16 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     }
     __syncthreads();
     if (sAbort) return;
-    // the metric record: normals (rounded once to the arithmetic type) and Jac
-    for (int k = tid; k < ncl * ML::kSize; k += NT) {
-        const int c = k / ML::kSize, o = k - c * ML::kSize;
-        const double v = sMetRaw[k];
-        if (o < NM) sNrm[c * NM + o] = (R)v;
-        else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
+    if (!split) {
+        // the metric record: normals (rounded once to the arithmetic type) and Jac
+        for (int k = tid; k < ncl * ML::kSize; k += NT) {
+            const int c = k / ML::kSize, o = k - c * ML::kSize;
+            const double v = sMetRaw[k];
+            if (o < NM) sNrm[c * NM + o] = (R)v;
+            else if (o < NM + NN) sJac[c * NJ + (o - NM)] = v;
+        }
+        __syncthreads();
     }
-    __syncthreads();
 
     // ---- A: interpolate every line to its flux points ---------------------------
     for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
@@ -423,9 +468,17 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = pr == N ? -1 : 1;
             } else {
-                const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
-                n0 = (R)__ldg(pn);
-                n1 = (R)__ldg(pn + 1);
+                // the left (partner) cell's normal, from the split array or
+                // the packed record
+                if (split) {
+                    const R *pn = reinterpret_cast<const R *>(a.nrm) + (size_t)pc * NM + ML::normal(pfam, pline, pr);
+                    n0 = __ldg(pn);
+                    n1 = __ldg(pn + 1);
+                } else {
+                    const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
+                    n0 = (R)__ldg(pn);
+                    n1 = (R)__ldg(pn + 1);
+                }
                 sign_l = pr == 0 ? -1 : 1;
                 sign_r = r == N ? -1 : 1;
             }
@@ -482,12 +535,21 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     __syncthreads();
 
     // ---- C: B gradient, sources and the residual per solution point ------------
+    // in a time step the RK coefficients of the stage (phase E runs here)
+    double cf[6];
+    if constexpr (!DIAG) {
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            const double dt = a.cases ? a.cases[cs].dt : a.dt;
+            cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
+        }
+    }
     double part_r = 0.0, part_d = 0.0;
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
         const int cell = c0 + c;
         const R *met = sNrm + c * NM;
-        const double J = sJac[c * NN + i + N * j];
+        const double J = sJac[c * NJ + i + N * j];
         const R *Fx = sF + c * S::kF + (0 * N + j) * NP * 9;  // xi-line j
         const R *Fy = sF + c * S::kF + (1 * N + i) * NP * 9;  // eta-line i
         const R *Vx = sV + c * S::kV + (0 * N + j) * NP * NG;
@@ -539,7 +601,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             }
         }
         const double divB = gB[0][0] + gB[1][1];
-        {
+        if constexpr (DIAG) {
             const double d = gB[1][0] - gB[0][1];
             sJz[c * NN + i + N * j] = d * d;
         }
@@ -585,16 +647,47 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             for (int k = 0; k < 9; k++) part_r += res[k] * res[k];
             part_d += divB * divB;
         }
-        // stage the residual; the RK update runs element-wise below
-        double *rs = sRes + c * NQ + 9 * (i + N * j);
+        double *ap = sA + c * NQ + 9 * (i + N * j);
+        if constexpr (DIAG) {
+            // stage the residual for phase E's copy-out
 #pragma unroll
-        for (int k = 0; k < 9; k++) rs[k] = res[k];
+            for (int k = 0; k < 9; k++) ap[k] = res[k];
+        } else {
+            // ---- E: the RK stage update of this point (iterations.f90:88-213);
+            // the point's state and RK register slot are read by this thread
+            // only, so the output goes to the register slot in place, and in
+            // the float form a float copy over the state slot for phase F
+            // element by element in order: float copy k overwrites bytes of
+            // state element k/2 <= k, already read
+            const size_t g = (size_t)cell * NQ + 9 * (i + N * j);
+            const int kind = a.rk_kind;
+            R *qf = reinterpret_cast<R *>(sQ + c * NQ + 9 * (i + N * j));
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                const double qk = q[k], r = res[k];
+                double o;
+                switch (kind) {
+                case kRkAxpy: o = qk + cf[0] * r; break;
+                case kRkTwoReg: o = (cf[1] * ap[k] + cf[2] * qk) + cf[0] * r; break;
+                case kRkTwoRegT: o = (cf[1] * ap[k] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
+                default:
+                    o = ((((cf[1] * a.reg_a[g + k] + cf[2] * a.reg_b[g + k]) + cf[3] * a.reg_c[g + k]) + cf[4] * qk) +
+                         cf[5] * a.reg_d[g + k]) +
+                        cf[0] * r;
+                    break;
+                }
+                ap[k] = o;
+                if (a.resid_w) a.resid_w[g + k] = r;
+                if constexpr (sizeof(R) != sizeof(double)) qf[k] = (R)o;
+            }
+            fence_proxy_async();  // sA is the source of the bulk store below
+        }
     }
     __syncthreads();
 
     // ---- D: AV smoothness sensor (comp_artificial_viscosity, AV.f90:14-83) ------
-    const bool av = a.artiv == 1 && a.vismode == 1;
-    if (av) {
+    const bool av = DIAG && a.artiv == 1 && a.vismode == 1;
+    if constexpr (DIAG) if (av) {
         constexpr int NL = N - 1;
         // the sensed fields: density (v = 0) and Jz^2 (v = 1)
         auto field = [&](int c, int v, int is, int js) -> double {
@@ -676,58 +769,27 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         }
     }
 
-    // ---- E: RK stage update, element-wise and coalesced (iterations.f90) -------
+    // ---- E: residual copy-out (residual evaluation) or the output store ---------
+    const double *qout_src = nullptr;
+    bool out_bulk = false;
     {
         const size_t g0 = (size_t)c0 * NQ;
         const int n = ncl * NQ;
         if constexpr (DIAG) {
             if (a.resid_out)
-                for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sRes[e];
+                for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sA[e];
         } else {
-            double cf[6];
-#pragma unroll
-            for (int i = 0; i < 6; i++) {
-                const double dt = a.cases ? a.cases[cs].dt : a.dt;
-                cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
+            // the output slice (formed in sA by phase C) to q_out: one bulk
+            // store issued by one thread, read from shared memory while phase
+            // F runs, or coalesced stores when the slice is not 16-byte aligned
+            double *dst = a.q_out + g0;
+            out_bulk = (((uintptr_t)dst | (size_t)n * sizeof(double)) & 15) == 0;
+            if (out_bulk) {
+                if (tid == 0) bulk_s2g(dst, sA, (unsigned)(n * sizeof(double)));
+            } else {
+                for (int e = tid; e < n; e += NT) dst[e] = sA[e];
             }
-            // the register reads of kU elements are issued before their use
-            constexpr int kU = 4;
-            const int kind = a.rk_kind;
-            for (int e0 = tid; e0 < n; e0 += kU * NT) {
-                double ra[kU], rb[kU], rc[kU], rd[kU];
-#pragma unroll
-                for (int u = 0; u < kU; u++) {
-                    const int e = e0 + u * NT;
-                    const size_t g = g0 + (e < n ? e : 0);
-                    ra[u] = kind != kRkAxpy ? a.reg_a[g] : 0.0;
-                    rb[u] = kind == kRkFive ? a.reg_b[g] : 0.0;
-                    rc[u] = kind == kRkFive ? a.reg_c[g] : 0.0;
-                    rd[u] = kind == kRkFive ? a.reg_d[g] : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < kU; u++) {
-                    const int e = e0 + u * NT;
-                    if (e >= n) break;
-                    const size_t g = g0 + e;
-                    const double q = sQ[e], r = sRes[e];
-                    double o;
-                    switch (kind) {
-                    case kRkAxpy: o = q + cf[0] * r; break;
-                    case kRkTwoReg: o = (cf[1] * ra[u] + cf[2] * q) + cf[0] * r; break;
-                    case kRkTwoRegT: o = (cf[1] * ra[u] + cf[2] * q) + (cf[0] * r) * cf[3]; break;
-                    default:
-                        o = ((((cf[1] * ra[u] + cf[2] * rb[u]) + cf[3] * rc[u]) + cf[4] * q) + cf[5] * rd[u]) +
-                            cf[0] * r;
-                        break;
-                    }
-                    a.q_out[g] = o;
-                    if (a.resid_w) a.resid_w[g] = r;
-                    sQ[e] = o;  // the sensor read sQ before the barrier above
-                    // the float form keeps the output in its arithmetic type for
-                    // phase F (the flux buffer is free by now)
-                    if constexpr (sizeof(R) != sizeof(double)) reinterpret_cast<R *>(sF)[e] = (R)o;
-                }
-            }
+            qout_src = sA;
         }
     }
 
@@ -739,9 +801,13 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
             int fam, line, r;
             face_point<N>(lf, nfp, fam, line, r);
-            const R *q = (sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(sQ) : reinterpret_cast<const R *>(sF)) +
-                         c * NQ + (fam == 0 ? 9 * N * line : 9 * line);
-            const int stride = fam == 0 ? 9 : 9 * N;
+            // the output state: sA (double), or its float copy over the
+            // state slots (9 floats at the start of each point's 9 doubles)
+            constexpr int PS = sizeof(R) == sizeof(double) ? 9 : 18;  // R per point
+            const R *q = (sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(qout_src)
+                                                      : reinterpret_cast<const R *>(sQ)) +
+                         c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
+            const int stride = fam == 0 ? PS : PS * N;
             R *o = to + (size_t)t * 9;
 #pragma unroll
             for (int k = 0; k < 9; k++) {
@@ -794,6 +860,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 a.cta_max[2 * blockIdx.x] = m0;
                 a.cta_max[2 * blockIdx.x + 1] = m1;
             }
+            // the bulk store must have read sA before the CTA's shared memory goes
+            if (out_bulk) bulk_wait_read();
         }
     }
 }
