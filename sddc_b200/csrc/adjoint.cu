@@ -310,9 +310,12 @@ int forward_steps(sddc_ctx *ctx, double dt, int step0, int nsteps, double *const
             a.slot_r = g;
             a.slot_w = g + 1;
             a.cta_max = cmax + (size_t)(5 * m + k) * 2 * fgrid;
-            if (!ctx->nrm_double) {  // the exact kernel reads double normals: convert the packed record
+            if (!ctx->nrm_double || ctx->jac_inv) {
+                // the exact kernel reads double normals and Jac itself: convert
+                // the packed record
                 a.nrm = nullptr;
                 a.jac = nullptr;
+                a.jac_inv = 0;
             }
             CKA(launch_stage_exact(ctx->N, ctx->cpb, false, a, ctx->ops, ctx->stream));
         }

@@ -232,6 +232,7 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
     const int diag_grid = (p->ncell + 7) / 8;
     const int mon_blocks = std::max(ctx->grid, diag_grid);
     ctx->nrm_double = p->precision != SDDC_MIXED;
+    ctx->jac_inv = p->precision != SDDC_FP64_EXACT;
     const size_t n_nrm = nc * 4 * p->N * (p->N + 1), n_jac = nc * ((p->N * p->N + 1) & ~1);
     if ((rc = alloc(ctx, (void **)&ctx->met, nc * ctx->msize * sizeof(double), "metrics")) ||
         (rc = alloc(ctx, &ctx->nrm, n_nrm * (ctx->nrm_double ? sizeof(double) : sizeof(float)), "normals")) ||
@@ -314,7 +315,8 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
         for (int k = 0; k < N * N; k++) m[kJac + k] = Jac[k + (size_t)N * N * c];
     }
     // the same, split: normals (rounded once to the form's type) and Jac
-    // padded to an even count, so that a tile's slices are 16-byte aligned
+    // (its IEEE reciprocal for the forms that multiply by 1/Jac) padded to
+    // an even count, so that a tile's slices are 16-byte aligned
     const int NJ = (N * N + 1) & ~1;
     std::vector<double> nrm_d, jac((size_t)NC * NJ, 0.0);
     std::vector<float> nrm_f;
@@ -326,7 +328,7 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
             if (ctx->nrm_double) nrm_d[c * kJac + o] = m[o];
             else nrm_f[c * kJac + o] = (float)m[o];
         }
-        for (int k = 0; k < N * N; k++) jac[c * NJ + k] = m[kJac + k];
+        for (int k = 0; k < N * N; k++) jac[c * NJ + k] = ctx->jac_inv ? 1.0 / m[kJac + k] : m[kJac + k];
     }
     // per-(cell, local face) records from the reference's face lists
     std::vector<int2> fr((size_t)NC * 4, make_int2(-1, 0));
@@ -471,6 +473,7 @@ StageArgs sddc::base_args(sddc_ctx *ctx)
     a.met = ctx->met;
     a.nrm = ctx->nrm;
     a.jac = ctx->jac;
+    a.jac_inv = ctx->jac_inv ? 1 : 0;
     a.faces = ctx->faces;
     a.maxima = ctx->maxima;
     a.sm_ind = ctx->sm_ind;

@@ -67,6 +67,7 @@ struct sddc_ctx {
     void *nrm = nullptr;
     double *jac = nullptr;
     bool nrm_double = true;  // normals stored as double (FP64 forms)
+    bool jac_inv = false;    // jac holds 1/Jac (the forms other than the exact one)
     int2 *faces = nullptr;
     double *maxima = nullptr;  // [sddc::kSlots][2]
     double *sm_ind = nullptr, *muav = nullptr, *resid = nullptr, *grad = nullptr;

@@ -103,6 +103,7 @@ struct StageArgs {
     // kernel converts the packed record
     const void *__restrict__ nrm;
     const double *__restrict__ jac;
+    int jac_inv;                       // jac holds 1/Jac (the forms other than the exact one)
     const int2 *__restrict__ faces;    // (cell, local face) records
     double *maxima;                    // [5][2]: running max of eigv, umax
     double *__restrict__ sm_ind;       // (2,NCELL) AV sensor
@@ -549,7 +550,14 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         const int i = t % N, j = (t / N) % N, c = t / NN;
         const int cell = c0 + c;
         const R *met = sNrm + c * NM;
-        const double J = sJac[c * NJ + i + N * j];
+        // Jac, or its reciprocal when the split array holds reciprocals (the
+        // exact form divides by Jac, as the reference does; the others multiply
+        // by 1/Jac, rounded once, on the host or here)
+        const double Jv = sJac[c * NJ + i + N * j];
+        double J = Jv, rJ = Jv;
+        if constexpr (!EX) {
+            if (!a.jac_inv) rJ = 1.0 / Jv;
+        }
         const R *Fx = sF + c * S::kF + (0 * N + j) * NP * 9;  // xi-line j
         const R *Fy = sF + c * S::kF + (1 * N + i) * NP * 9;  // eta-line i
         const R *Vx = sV + c * S::kV + (0 * N + j) * NP * NG;
@@ -585,7 +593,6 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 gx = (double)(ax + bx) / J;
                 gy = (double)(ay + by) / J;
             } else {
-                const double rJ = 1.0 / J;
                 gx = (double)(ax + bx) * rJ;
                 gy = (double)(ay + by) * rJ;
             }
@@ -622,7 +629,6 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int k = 0; k < 9; k++) res[k] = res[k] / J;
         } else {
-            const double rJ = 1.0 / J;
 #pragma unroll
             for (int k = 0; k < 9; k++) res[k] = res[k] * rJ;
         }
