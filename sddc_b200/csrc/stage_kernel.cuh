@@ -256,6 +256,12 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     stage_kernel(const StageArgs a, const Ops ops)
 {
     constexpr bool EX = EXACT && (sizeof(R) == sizeof(double));
+    // a time step of the forms other than the exact one needs only div B:
+    // the face-averaged state is kept as its contravariant component
+    // Bn = Bx n0 + By n1 at each flux point (this cell's normal), and div B
+    // is the SD divergence of Bn (the same sum as the exact form's
+    // d(Bx)/dx + d(By)/dy, associated differently)
+    constexpr bool kBn = !DIAG && !EX;
     using S = Smem<N, R, DIAG>;
     using ML = MetLayout<N>;
     constexpr int NT = stage_threads(N, CPB);  // whole warps: the reductions use full-warp masks
@@ -434,8 +440,12 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int k = 0; k < 9; k++) vs[k] = q[k];
         } else {
-            vs[0] = q[5];
-            vs[1] = q[6];
+            if constexpr (kBn) {
+                vs[0] = q[5] * n0 + q[6] * n1;
+            } else {
+                vs[0] = q[5];
+                vs[1] = q[6];
+            }
         }
     }
 
@@ -509,8 +519,13 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
 #pragma unroll
             for (int k = 0; k < 9; k++) vs[k] = (R)0.5 * Ql[k] + (R)0.5 * Qr[k];
         } else {
-            vs[0] = (R)0.5 * Ql[5] + (R)0.5 * Qr[5];
-            vs[1] = (R)0.5 * Ql[6] + (R)0.5 * Qr[6];
+            const R bxa = (R)0.5 * Ql[5] + (R)0.5 * Qr[5], bya = (R)0.5 * Ql[6] + (R)0.5 * Qr[6];
+            if constexpr (kBn) {
+                vs[0] = bxa * onrm[0] + bya * onrm[1];  // this cell's normal
+            } else {
+                vs[0] = bxa;
+                vs[1] = bya;
+            }
         }
     }
     __syncthreads();
@@ -572,9 +587,21 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 for (int k = 0; k < 18; k++) go[k] = 0.0;
             }
         }
+        double divB = 0.0;
+        if constexpr (kBn) {
+            // div B from the contravariant component Bn at the flux points
+            if (a.vismode == 1) {
+                R sx = (R)0, sy = (R)0;
+#pragma unroll
+                for (int r = 0; r < NP; r++) sx = sx + Vx[r * NG] * sOpM[r * N + i];
+#pragma unroll
+                for (int r = 0; r < NP; r++) sy = sy + Vy[r * NG] * sOpM[r * N + j];
+                divB = (double)(sx + sy) * rJ;
+            }
+        }
 #pragma unroll
         for (int g = 0; g < NG; g++) {
-            if (a.vismode != 1) break;
+            if (kBn || a.vismode != 1) break;
             R ax = (R)0, ay = (R)0, bx = (R)0, by = (R)0;
 #pragma unroll
             for (int r = 0; r < NP; r++) {
@@ -607,7 +634,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 }
             }
         }
-        const double divB = gB[0][0] + gB[1][1];
+        if constexpr (!kBn) divB = gB[0][0] + gB[1][1];
         if constexpr (DIAG) {
             const double d = gB[1][0] - gB[0][1];
             sJz[c * NN + i + N * j] = d * d;
