@@ -439,16 +439,28 @@ def ensemble_run(torch, ncase=64, steps=20, warmup=3, seed=0):
     qb = b.solver.state()["Q"]
     finite = bool(np.isfinite(qb).all())
     b.close()
-    t_seq = 0.0
     from sddc_b200.solver import Solver
 
+    # each case on its own context, one after another: the mixed form, and
+    # the FP64 drop-in in both FP64 forms; the exact form's final states (bit
+    # for bit the oracle's) are the reference of the batch's accuracy
+    t_seq = {"mixed": 0.0, "fp64": 0.0, "fp64_exact": 0.0}
+    errs = []
+    off = 0
     for m in members:
-        cpb, _ = autotune.tune(m.tables, m.case.physics, m.Q0, m.dt, "mixed", steps=2)
-        s = Solver(m.tables, m.case.physics, precision="mixed", cells_per_cta=cpb)
-        s.set_state(m.Q0)
-        s.rk_s5p3(m.dt, warmup)
-        t_seq += timed(lambda: s.rk_s5p3(m.dt, steps), s.stream_handle())
-        s.close()
+        nq = m.Q0.size
+        for prec in t_seq:
+            cpb, _ = autotune.tune(m.tables, m.case.physics, m.Q0, m.dt, prec, steps=2)
+            s = Solver(m.tables, m.case.physics, precision=prec, cells_per_cta=cpb)
+            s.set_state(m.Q0)
+            s.rk_s5p3(m.dt, warmup)
+            t_seq[prec] += timed(lambda: s.rk_s5p3(m.dt, steps), s.stream_handle())
+            if prec == "fp64_exact":
+                ref = s.state()["Q"].ravel(order="F")
+                got = qb.ravel(order="F")[off:off + nq]
+                errs.append(float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+            s.close()
+        off += nq
     units = dof_total * 5 * steps
     sizes = {}
     for m in members:
@@ -457,8 +469,15 @@ def ensemble_run(torch, ncase=64, steps=20, warmup=3, seed=0):
     return {"cases": ncase, "dof_total": dof_total, "cells_by_case_size": sizes, "steps": steps,
             "form": "mixed", "cells_per_cta": best, "finite": finite,
             "batched": {"value": units / t_batch, "unit": UNIT, "s_per_step": t_batch / steps},
-            "sequential": {"value": units / t_seq, "unit": UNIT, "s_per_step": t_seq / steps},
-            "batched_over_sequential": t_seq / t_batch}
+            "sequential": {"value": units / t_seq["mixed"], "unit": UNIT, "s_per_step": t_seq["mixed"] / steps},
+            "batched_over_sequential": t_seq["mixed"] / t_batch,
+            "fp64_dropin": {f: {"value": units / t_seq[f], "unit": UNIT, "s_per_step": t_seq[f] / steps}
+                            for f in ("fp64", "fp64_exact")},
+            "batched_mixed_over_fp64_dropin": t_seq["fp64"] / t_batch,
+            "batched_mixed_over_fp64_exact_dropin": t_seq["fp64_exact"] / t_batch,
+            "batched_mixed_rel_l2_vs_exact": {"max": max(errs), "median": float(np.median(errs)),
+                                              "after_steps": warmup + steps,
+                                              "note": "per case, against the exact form (bit-equal to the oracle)"}}
 
 
 def output_bench(torch, solver_mod, mesh, t, ph, Q0, dt, cpb, steps=200, nwrite=100, nre=4):
