@@ -56,7 +56,7 @@ struct VjpArgs {
     double alpha, c_h;
     Freestream fs;
     const double *__restrict__ q;     // stage input state (9,N,N,NCELL)
-    const double *__restrict__ t_in;  // its face traces [cell][lf][nfp][9]
+    const double *__restrict__ t_in;  // its face traces, layout trace_at
     const double *xbar;               // adjoint of the stage output; null: objective seeds only
     double lam_scale;                 // lambda = lam_scale * xbar
     const double *__restrict__ at;    // adjoint traces [cell][lf][nfp][12]
@@ -340,9 +340,8 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
         const bool own_right = kind == kFaceRight;
         if (kind == kFaceLeft || own_right) {
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
-            const double *tp = a.t_in + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 9;
 #pragma unroll
-            for (int k = 0; k < 9; k++) oth[k] = tp[k];
+            for (int k = 0; k < 9; k++) oth[k] = a.t_in[trace_at<N>(pc, plf, N - nfp, k)];
         } else {
             const double *nrm = sNrm + c * NM + ML::normal(fam, line, r);
             bc_ghost<double, true>(kind, own, nrm[0], nrm[1], a.vismode, a.fs, oth);
@@ -716,8 +715,7 @@ __global__ void __launch_bounds__(128) adj_locate_kernel(const LocateArgs a, con
                 const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
                 int pfam, pline, pr;
                 face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
-                const double *tp = a.t_in + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 9;
-                for (int k = 0; k < 9; k++) oth[k] = tp[k];
+                for (int k = 0; k < 9; k++) oth[k] = a.t_in[trace_at<N>(pc, plf, N - nfp, k)];
                 if (!own_right) {
                     sign_r = pr == N ? -1 : 1;
                 } else {
@@ -776,11 +774,11 @@ __global__ void __launch_bounds__(256) wall_force_kernel(int nw, const int2 *__r
         const int nfp = 1 + e % N, lf = wf.y;
         int fam, line, r;
         face_point<N>(lf, nfp, fam, line, r);
-        const double *own = t + (((size_t)wf.x * 4 + (lf - 1)) * N + (nfp - 1)) * 9;
+        const size_t own = trace_at<N>(wf.x, lf, nfp - 1, 0);  // variable k at own + k*N
         const double *nr = met + (size_t)wf.x * ML::kSize + ML::normal(fam, line, r);
         const int sign_l = r == 0 ? -1 : 1;
         double ql[9], gh[9], Fl[9], Fr[9], eig, um = 0.0;
-        for (int k = 0; k < 9; k++) ql[k] = own[k];
+        for (int k = 0; k < 9; k++) ql[k] = t[own + (size_t)k * N];
         bc_ghost<double, true>(kFaceWall, ql, nr[0], nr[1], vismode, fs, gh);
         rusanov<double, true>(ql, gh, Fl, Fr, nr[0], nr[1], sign_l, 1, 0.0, eig, um);
         const double w = wq[line] * (double)sign_l;

@@ -90,7 +90,7 @@ struct StageArgs {
     const CaseParams *cases;
     const double *__restrict__ q_in;   // (9,N,N,NCELL), never written during the stage
     double *q_out;                     // RK output (may be reg_a: FiveStageRk stage 5)
-    const void *__restrict__ t_in;     // face traces of q_in, R[NCELL][4][N][9]
+    const void *__restrict__ t_in;     // face traces of q_in, R[NCELL][4][9][N] (trace_at)
     void *t_out;                       // face traces of q_out (null: not produced)
     const double *reg_a;               // RK registers read by this stage
     const double *reg_b;
@@ -209,6 +209,14 @@ __device__ __forceinline__ void face_point(int lf, int nfp, int &fam, int &line,
     case 3: fam = 1; line = N - nfp; r = N; break;       // (N-nfp+1, N+1)
     default: fam = 0; line = N - nfp; r = 0; break;      // (1, N-nfp+1)
     }
+}
+
+// face traces of a state, [cell][local face][variable][face point]: the N
+// points of one face, which consecutive lanes read and write, are adjacent.
+// lf is 1-based, nfp0 0-based.
+template <int N> __host__ __device__ __forceinline__ size_t trace_at(size_t cell, int lf, int nfp0, int k)
+{
+    return ((cell * 4 + (size_t)(lf - 1)) * 9 + (size_t)k) * N + (size_t)nfp0;
 }
 
 template <typename T> __device__ __forceinline__ T warp_max(T v)
@@ -471,9 +479,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
             int pfam, pline, pr;
             face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
-            const R *tp = reinterpret_cast<const R *>(a.t_in) + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 9;
+            const R *tp = reinterpret_cast<const R *>(a.t_in);
 #pragma unroll
-            for (int k = 0; k < 9; k++) other[k] = tp[k];
+            for (int k = 0; k < 9; k++) other[k] = tp[trace_at<N>(pc, plf, N - nfp, k)];
             if (!own_right) {
                 n0 = onrm[0]; n1 = onrm[1];
                 sign_l = r == 0 ? -1 : 1;
@@ -829,7 +837,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     // ---- F: face traces of the output state for the next stage's neighbours ---
     if (!DIAG && a.t_out) {
         __syncthreads();
-        R *to = reinterpret_cast<R *>(a.t_out) + (size_t)c0 * 4 * N * 9;
+        R *to = reinterpret_cast<R *>(a.t_out);
         for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
             const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
             int fam, line, r;
@@ -841,13 +849,12 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                                                       : reinterpret_cast<const R *>(sQ)) +
                          c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
             const int stride = fam == 0 ? PS : PS * N;
-            R *o = to + (size_t)t * 9;
 #pragma unroll
             for (int k = 0; k < 9; k++) {
                 R acc = (R)0;
 #pragma unroll
                 for (int s = 0; s < N; s++) acc = acc + (R)q[k + stride * s] * sOpL[r * N + s];
-                o[k] = acc;
+                to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
             }
         }
     }
@@ -899,15 +906,16 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     }
 }
 
-// Face traces of a state: T[cell][lf][nfp][k] = sum_s Q(k, line points) *
-// L(r, s) at the flux point of local face lf, face point nfp -- the same
-// interpolation, in the same order and type, as phase A and phase F.
+// Face traces of a state: T[trace_at(cell, lf, nfp, k)] = sum_s Q(k, line
+// points) * L(r, s) at the flux point of local face lf, face point nfp -- the
+// same interpolation, in the same order and type, as phase A and phase F.
 template <int N, typename R, bool EXACT>  // EXACT: compiled with -fmad=false, like phase A
 __global__ void trace_kernel(int ncell, const double *__restrict__ q, R *__restrict__ t, const Ops ops)
 {
     const size_t n = (size_t)ncell * 4 * N * 9;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(e % 9), nfp = 1 + (int)((e / 9) % N), lf = 1 + (int)((e / (9 * N)) % 4);
+        // e = trace_at(c, lf, nfp - 1, k)
+        const int nfp = 1 + (int)(e % N), k = (int)((e / N) % 9), lf = 1 + (int)((e / (9 * N)) % 4);
         const size_t c = e / (36 * N);
         int fam, line, r;
         face_point<N>(lf, nfp, fam, line, r);

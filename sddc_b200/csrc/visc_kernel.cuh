@@ -39,7 +39,7 @@ struct ViscArgs {
     double mu, eta0;
     Freestream fs;
     const double *__restrict__ q;     // stage input state
-    const void *t_in;                 // its face traces [cell][lf][nfp][9], in the form's type
+    const void *t_in;                 // its face traces (layout trace_at), in the form's type
     const double *__restrict__ met;   // packed metrics
     const double *__restrict__ met2;  // [cell][lf][nfp][2]: S1(2,1:2) or S2(1,1:2) at the face point
     const int2 *__restrict__ faces;
@@ -172,9 +172,9 @@ __device__ __forceinline__ void visc_stage_states(const ViscArgs &a, const Ops &
         const bool own_right = kind == kFaceRight;
         if (kind == kFaceLeft || own_right) {
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
-            const T *tp = reinterpret_cast<const T *>(a.t_in) + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 9;
+            const T *tp = reinterpret_cast<const T *>(a.t_in);
 #pragma unroll
-            for (int k = 0; k < 9; k++) oth[k] = (double)tp[k];
+            for (int k = 0; k < 9; k++) oth[k] = (double)tp[trace_at<N>(pc, plf, N - nfp, k)];
         } else {
             const double *nrm = sNrm + c * NM + ML::normal(fam, line, r);
             bc_ghost<double, true>(kind, own, nrm[0], nrm[1], a.vismode, a.fs, oth);
