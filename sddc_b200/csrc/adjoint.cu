@@ -36,7 +36,7 @@ namespace sddc {
 
 struct AdjWs {
     int grid = 0;            // VJP CTAs
-    double *at = nullptr;    // adjoint traces [ncell][4N][12]
+    double *at = nullptr;    // adjoint traces, ncell * 4N * 12 (adj_trace_at)
     double *part = nullptr;  // [grid][8]
     AdjScalars *acc = nullptr;
     AdjRec *recs = nullptr;

@@ -59,7 +59,7 @@ struct VjpArgs {
     const double *__restrict__ t_in;  // its face traces, layout trace_at
     const double *xbar;               // adjoint of the stage output; null: objective seeds only
     double lam_scale;                 // lambda = lam_scale * xbar
-    const double *__restrict__ at;    // adjoint traces [cell][lf][nfp][12]
+    const double *__restrict__ at;    // adjoint traces, layout adj_trace_at
     const double *__restrict__ met;
     const int2 *__restrict__ faces;
     // epilogue: out = (wa*ra + wb*rb) + qbar;  out2 = wc*rc + wd*xbar
@@ -87,11 +87,19 @@ template <int N, int CPB> constexpr size_t vjp_smem_doubles()
 }
 
 // ---- adjoint traces ----------------------------------------------------------
-// at[cell][lf][nfp] = (Fbar(9), Vbar_Bx, Vbar_By, 0): the adjoint of this
+// at(cell, lf, nfp) = (Fbar(9), Vbar_Bx, Vbar_By, 0): the adjoint of this
 // cell's flux value at the face point (from the divergence, compresid.f90:
 // 12-51) and of the face-averaged Bx, By (from divB in the Powell source,
 // compresid.f90:58, through nablaQsp compflux.f90:107-157).
 constexpr int kTraceCpb = 8;  // cells per CTA of adj_trace_kernel
+
+// adjoint trace layout, [cell][local face][value][face point] like trace_at:
+// the N points of a face, which consecutive lanes write and read, are
+// adjacent (lf 1-based, nfp0 0-based, 12 values, the last one 0)
+template <int N> __host__ __device__ __forceinline__ size_t adj_trace_at(size_t cell, int lf, int nfp0, int k)
+{
+    return ((cell * 4 + (size_t)(lf - 1)) * 12 + (size_t)k) * N + (size_t)nfp0;
+}
 
 template <int N>
 __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, const double *__restrict__ xbar,
@@ -171,12 +179,11 @@ __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, 
             bs += m * sB[c * NN + sp];
         }
         const double *nr = met + (size_t)(c0 + c) * ML::kSize + ML::normal(fam, line, r);
-        double *o = at + ((size_t)c0 * 4 * N + t) * 12;
 #pragma unroll
-        for (int k = 0; k < 9; k++) o[k] = fb[k];
-        o[9] = bs * nr[0];
-        o[10] = bs * nr[1];
-        o[11] = 0.0;
+        for (int k = 0; k < 9; k++) at[adj_trace_at<N>(c0 + c, lf, nfp - 1, k)] = fb[k];
+        at[adj_trace_at<N>(c0 + c, lf, nfp - 1, 9)] = bs * nr[0];
+        at[adj_trace_at<N>(c0 + c, lf, nfp - 1, 10)] = bs * nr[1];
+        at[adj_trace_at<N>(c0 + c, lf, nfp - 1, 11)] = 0.0;
     }
 }
 
@@ -501,12 +508,11 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
 #pragma unroll
                 for (int k = 0; k < 9; k++) fbar[k] = ms * fown[k];
                 if (a.xbar) {
-                    const double *ap = a.at + (((size_t)pc * 4 + (plf - 1)) * N + (N - nfp)) * 12;
 #pragma unroll
-                    for (int k = 0; k < 9; k++) fbar[k] += ps * ap[k];
+                    for (int k = 0; k < 9; k++) fbar[k] += ps * a.at[adj_trace_at<N>(pc, plf, N - nfp, k)];
                     if (a.vismode == 1) {
-                        vbx += ap[9];
-                        vby += ap[10];
+                        vbx += a.at[adj_trace_at<N>(pc, plf, N - nfp, 9)];
+                        vby += a.at[adj_trace_at<N>(pc, plf, N - nfp, 10)];
                     }
                 }
             } else {
@@ -558,15 +564,34 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     __syncthreads();
 
     // ---- RK reverse update, element-wise ----------------------------------------------
+    // the register reads of kU elements are issued before their use, so that
+    // each thread keeps several loads in flight
     {
+        constexpr int kU = 4;
         const size_t g0 = (size_t)c0 * NQ;
-        for (int e = tid; e < ncl * NQ; e += NT) {
-            const size_t g = g0 + e;
-            double o = 0.0;
-            if (a.ra) o = a.wa * a.ra[g];
-            if (a.rb) o = o + a.wb * a.rb[g];
-            a.out[g] = o + sQ[e];
-            if (a.out2) a.out2[g] = (a.rc ? a.wc * a.rc[g] : 0.0) + a.wd * a.xbar[g];
+        const int n = ncl * NQ;
+        for (int e0 = tid; e0 < n; e0 += kU * NT) {
+            double va[kU], vb[kU], vc[kU], vx[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int e = e0 + u * NT;
+                const size_t g = g0 + (e < n ? e : 0);
+                va[u] = a.ra ? a.ra[g] : 0.0;
+                vb[u] = a.rb ? a.rb[g] : 0.0;
+                vc[u] = a.out2 && a.rc ? a.rc[g] : 0.0;
+                vx[u] = a.out2 ? a.xbar[g] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int e = e0 + u * NT;
+                if (e >= n) break;
+                const size_t g = g0 + e;
+                double o = 0.0;
+                if (a.ra) o = a.wa * va[u];
+                if (a.rb) o = o + a.wb * vb[u];
+                a.out[g] = o + sQ[e];
+                if (a.out2) a.out2[g] = (a.rc ? a.wc * vc[u] : 0.0) + a.wd * vx[u];
+            }
         }
     }
 
