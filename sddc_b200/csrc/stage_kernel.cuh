@@ -655,8 +655,13 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             const R dF = Fx[i * 9 + k], dG = Fy[j * 9 + k];
             res[k] = (double)(-(dF + dG));
             // the viscous chain (compresid.f90:34-49); it adds exactly +0.0
-            // when mu == eta0 == 0
-            if (a.vismode == 1) res[k] = res[k] + (a.visc ? a.visc[(size_t)cell * NQ + 9 * (i + N * j) + k] : 0.0);
+            // when mu == eta0 == 0, which only the exact form reproduces (it
+            // turns a -0.0 residual into +0.0)
+            if constexpr (EX) {
+                if (a.vismode == 1) res[k] = res[k] + (a.visc ? a.visc[(size_t)cell * NQ + 9 * (i + N * j) + k] : 0.0);
+            } else {
+                if (a.vismode == 1 && a.visc) res[k] = res[k] + a.visc[(size_t)cell * NQ + 9 * (i + N * j) + k];
+            }
         }
         // compresid.f90:53-78: 1/Jac, Powell 8-wave and GLM sources
         const double *q = sQ + c * NQ + 9 * (i + N * j);
@@ -838,23 +843,51 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     if (!DIAG && a.t_out) {
         __syncthreads();
         R *to = reinterpret_cast<R *>(a.t_out);
-        for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
-            const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
-            int fam, line, r;
-            face_point<N>(lf, nfp, fam, line, r);
-            // the output state: sA (double), or its float copy over the
-            // state slots (9 floats at the start of each point's 9 doubles)
-            constexpr int PS = sizeof(R) == sizeof(double) ? 9 : 18;  // R per point
-            const R *q = (sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(qout_src)
-                                                      : reinterpret_cast<const R *>(sQ)) +
-                         c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
-            const int stride = fam == 0 ? PS : PS * N;
+        // the output state: sA (double), or its float copy over the state
+        // slots (9 floats at the start of each point's 9 doubles)
+        constexpr int PS = sizeof(R) == sizeof(double) ? 9 : 18;  // R per point
+        const R *qo = sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(qout_src)
+                                                  : reinterpret_cast<const R *>(sQ);
+        if constexpr (sizeof(R) == sizeof(double)) {
+            // one thread per (cell, family, variable, line): the line's N
+            // values give the traces at both of its ends (r = 0 and r = N),
+            // each summed in order as phase A sums them (measured faster than
+            // one thread per face point in the FP64 forms, slower in the mixed)
+            for (int t = tid; t < ncl * 2 * 9 * N; t += NT) {
+                const int line = t % N, k = (t / N) % 9, fam = (t / (9 * N)) % 2, c = t / (18 * N);
+                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line) + k;
+                const int stride = fam == 0 ? PS : PS * N;
+                R qs[N];
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
-                R acc = (R)0;
+                for (int s = 0; s < N; s++) qs[s] = q[stride * s];
+                R a0 = (R)0, aN = (R)0;
 #pragma unroll
-                for (int s = 0; s < N; s++) acc = acc + (R)q[k + stride * s] * sOpL[r * N + s];
-                to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
+                for (int s = 0; s < N; s++) {
+                    a0 = a0 + qs[s] * sOpL[s];
+                    aN = aN + qs[s] * sOpL[N * N + s];
+                }
+                // the faces at the line's ends (face_point inverted): xi line j
+                // ends on local faces 4 (point N-j) and 2 (point j+1), eta
+                // line i on local faces 1 (point i+1) and 3 (point N-i)
+                const int lf0 = fam == 0 ? 4 : 1, nfp0 = fam == 0 ? N - line : line + 1;
+                const int lfN = fam == 0 ? 2 : 3, nfpN = fam == 0 ? line + 1 : N - line;
+                to[trace_at<N>(c0 + c, lf0, nfp0 - 1, k)] = a0;
+                to[trace_at<N>(c0 + c, lfN, nfpN - 1, k)] = aN;
+            }
+        } else {
+            for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
+                const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
+                int fam, line, r;
+                face_point<N>(lf, nfp, fam, line, r);
+                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
+                const int stride = fam == 0 ? PS : PS * N;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    R acc = (R)0;
+#pragma unroll
+                    for (int s = 0; s < N; s++) acc = acc + q[k + stride * s] * sOpL[r * N + s];
+                    to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
+                }
             }
         }
     }
