@@ -208,6 +208,10 @@ int reverse_stage(sddc_ctx *ctx, const RevStage &s)
     a.lam_scale = s.scale;
     a.at = w->at;
     a.met = ctx->met;
+    if (ctx->nrm_double && !ctx->jac_inv) {  // an exact context holds double normals and Jac
+        a.nrm = static_cast<const double *>(ctx->nrm);
+        a.jac = ctx->jac;
+    }
     a.faces = ctx->faces;
     a.ra = s.ra;
     a.rb = s.rb;

@@ -61,6 +61,9 @@ struct VjpArgs {
     double lam_scale;                 // lambda = lam_scale * xbar
     const double *__restrict__ at;    // adjoint traces, layout adj_trace_at
     const double *__restrict__ met;
+    // the split metrics of an exact context (double normals [NCELL][4N(N+1)],
+    // Jac [NCELL][MetLayout::kJacPad]), staged directly; null: the packed record
+    const double *__restrict__ nrm, *__restrict__ jac;
     const int2 *__restrict__ faces;
     // epilogue: out = (wa*ra + wb*rb) + qbar;  out2 = wc*rc + wd*xbar
     const double *ra, *rb;
@@ -83,7 +86,7 @@ template <int N, int CPB> constexpr size_t vjp_smem_doubles()
 {
     constexpr int NQ = 9 * N * N, NP = N + 1, NN = N * N;
     constexpr int kF = 2 * N * NP * 9, kV = 2 * N * NP * 2, kO = 4 * N * 9, NM = 2 * MetLayout<N>::kFam;
-    return (size_t)CPB * (2 * NQ + 2 * kF + kV + kO + 2 * NN + NM) + 2 * NP * N + 8 * 32;
+    return (size_t)CPB * (2 * NQ + 2 * kF + kV + kO + MetLayout<N>::kJacPad + NN + NM) + 2 * NP * N + 8 * 32;
 }
 
 // ---- adjoint traces ----------------------------------------------------------
@@ -258,8 +261,9 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     double *sFb = sQf + CPB * kF;                       // [CPB][2][N][NP][9] flux adjoint, then state adjoint
     double *sVb = sFb + CPB * kF;                       // [CPB][2][N][NP][2] face-averaged Bx,By, then adjoint
     double *sQo = sVb + CPB * kV;                       // [CPB][4N][9] neighbour / ghost trace
-    double *sJac = sQo + CPB * kO;                      // [CPB][NN]
-    double *sBeta = sJac + CPB * NN;                    // [CPB][NN] adjoint of divB, over Jac
+    constexpr int NJ = ML::kJacPad;
+    double *sJac = sQo + CPB * kO;                      // [CPB][NJ]
+    double *sBeta = sJac + CPB * NJ;                    // [CPB][NN] adjoint of divB, over Jac
     double *sNrm = sBeta + CPB * NN;                    // [CPB][NM]
     double *sL = sNrm + CPB * NM;                       // [NP][N]
     double *sM = sL + NP * N;                           // [NP][N]
@@ -270,22 +274,34 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     const int ncl = min(CPB, a.ncell - c0);
 
     // the tile's state, lambda source and metric slices by TMA bulk copies
-    // (the metric records land in sQf, free until the primal phase) when
-    // they are 16-byte aligned, else by loads
+    // when they are 16-byte aligned, else by loads: the split normals and Jac
+    // straight into place, or the packed metric records into sQf (free until
+    // the primal phase) for conversion
     __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sAbort;
+    const bool split = a.nrm != nullptr;  // uniform
     {
         const double *qsrc = a.q + (size_t)c0 * NQ, *msrc = a.met + (size_t)c0 * ML::kSize;
+        const double *nsrc = split ? a.nrm + (size_t)c0 * NM : nullptr, *jsrc = split ? a.jac + (size_t)c0 * NJ : nullptr;
         const double *xsrc = a.xbar ? a.xbar + (size_t)c0 * NQ : nullptr;
-        const size_t qbytes = (size_t)ncl * NQ * sizeof(double), mbytes = (size_t)ncl * ML::kSize * sizeof(double);
-        const bool bulk = (((uintptr_t)qsrc | (uintptr_t)msrc | (uintptr_t)xsrc | qbytes | mbytes) & 15) == 0;
+        const size_t qbytes = (size_t)ncl * NQ * sizeof(double);
+        const size_t mbytes = split ? 0 : (size_t)ncl * ML::kSize * sizeof(double);
+        const size_t nbytes = split ? (size_t)ncl * NM * sizeof(double) : 0;
+        const size_t jbytes = split ? (size_t)ncl * NJ * sizeof(double) : 0;
+        const bool bulk = (((uintptr_t)qsrc | (uintptr_t)msrc | (uintptr_t)nsrc | (uintptr_t)jsrc | (uintptr_t)xsrc |
+                            qbytes | mbytes | nbytes | jbytes) & 15) == 0;
         if (tid == 0) {
             sAbort = 0;
             if (bulk) {
                 mbar_init(&sBar, 1);
-                mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + (xsrc ? qbytes : 0)));
+                mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes + (xsrc ? qbytes : 0)));
                 bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
-                bulk_g2s(sQf, msrc, (unsigned)mbytes, &sBar);
+                if (split) {
+                    bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
+                    bulk_g2s(sJac, jsrc, (unsigned)jbytes, &sBar);
+                } else {
+                    bulk_g2s(sQf, msrc, (unsigned)mbytes, &sBar);
+                }
                 if (xsrc) bulk_g2s(sA, xsrc, (unsigned)qbytes, &sBar);
             }
         }
@@ -298,7 +314,12 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 sQ[k] = __ldg(qsrc + k);
                 if (xsrc) sA[k] = xsrc[k];
             }
-            for (int k = tid; k < ncl * ML::kSize; k += NT) sQf[k] = __ldg(msrc + k);
+            if (split) {
+                for (int k = tid; k < ncl * NM; k += NT) sNrm[k] = __ldg(nsrc + k);
+                for (int k = tid; k < ncl * NJ; k += NT) sJac[k] = __ldg(jsrc + k);
+            } else {
+                for (int k = tid; k < ncl * ML::kSize; k += NT) sQf[k] = __ldg(msrc + k);
+            }
         }
         if (bulk && tid == 0 && !mbar_wait_bounded(&sBar, 0)) {
             atomicOr(a.err, kErrStagingTimeout);  // the copies did not complete
@@ -309,12 +330,13 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     __syncthreads();
     if (sAbort) return;
     for (int k = tid; k < ncl * NQ; k += NT) sA[k] = a.xbar ? a.lam_scale * sA[k] : 0.0;
-    for (int k = tid; k < ncl * ML::kSize; k += NT) {
-        const int c = k / ML::kSize, o = k - c * ML::kSize;
-        const double v = sQf[k];
-        if (o < NM) sNrm[c * NM + o] = v;
-        else if (o < NM + NN) sJac[c * NN + (o - NM)] = v;
-    }
+    if (!split)
+        for (int k = tid; k < ncl * ML::kSize; k += NT) {
+            const int c = k / ML::kSize, o = k - c * ML::kSize;
+            const double v = sQf[k];
+            if (o < NM) sNrm[c * NM + o] = v;
+            else if (o < NM + NN) sJac[c * NJ + (o - NM)] = v;
+        }
     __syncthreads();
 
     // ---- primal: flux-point states (phase A of the stage kernel) ----------------
@@ -366,7 +388,7 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     // ---- per solution point: divB, the source adjoint, -lambda/J, divB adjoint ------
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
-        const double J = sJac[c * NN + i + N * j];
+        const double J = sJac[c * NJ + i + N * j];
         const double *met = sNrm + c * NM;
         double divB = 0.0;
         if (a.vismode == 1) {
