@@ -111,6 +111,8 @@ ALL_SMALL = {
     "periodic_n4": lambda: case_periodic(N=4),
     "wallbox_vis1": lambda: case_wall_box(vismode=1),
     "wallbox_vis0": lambda: case_wall_box(vismode=0),
+    "periodic_n2": lambda: case_periodic(N=2),
+    "cylinder_n6": lambda: case_cylinder(N=6),
     "cylinder_curved_n4": lambda: case_cylinder_curved(N=4),
     "wavybox_n5": lambda: case_wavy(N=5),
 }
