@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import sddc_oracle as O
-from helpers import ALL_SMALL, case_channel, case_cylinder, rel_l2
+from helpers import ALL_SMALL, case_channel, case_cylinder, channel_physics, rel_l2, smooth_state
 from sddc_b200 import cases, host, mesh
 from sddc_b200.solver import ENUMERIC, NumericalFault, SddcError, Solver
 
@@ -167,3 +167,25 @@ def test_sensor_after_rk_steps(name, k_stage):
     s.rk_s5p3(dt, 1)
     assert np.array_equal(s.state()["Q"], o.state()["Q"])
     assert s.maxima()["eigvmax"] == o.maxima()["eigvmax"]
+
+
+@pytest.mark.parametrize("nx,ny", [(1, 1), (3, 1), (1, 5)])
+@pytest.mark.parametrize("cpb", [4, 8])
+def test_minimal_meshes_exact(nx, ny, cpb):
+    """A single cell with four boundary faces, and single rows of cells: one
+    partial tile, every face of a cell on a boundary or on one neighbour."""
+    m = mesh.channel_box(nx, ny, sides=("WALL", "OUTL", "SYMP", "INLE"))
+    t = host.build_tables(m, 4)
+    ph = channel_physics(1)
+    Q = smooth_state(t, ph)
+    o = O.Oracle(t, ph, skip_ideal_viscous=False)
+    s = Solver(t, ph, precision="fp64_exact", cells_per_cta=cpb)
+    o.set_state(Q)
+    s.set_state(Q)
+    o.compresid()
+    s.compresid()
+    assert np.array_equal(s.state(resid=True)["resid"], o.state()["resid"])
+    o.rk_s5p3(1e-3, 3)
+    s.rk_s5p3(1e-3, 3)
+    assert np.array_equal(s.state()["Q"], o.state()["Q"])
+    s.close()
