@@ -15,6 +15,17 @@ Arms:
 * ``--impl reference``: the reference's own path on the CPU, i.e. the oracle
   restatement (the Fortran reference cannot be built here), all host cores.
 
+Blocks beside the headline, at N = 1 only (a flag skips each):
+* ``accuracy``: the mixed and FP64 forms against the exact form (bit-equal
+  to the oracle) over 2000 steps, per variable, with ||divB|| and mass drift;
+* ``ensemble``: 64 cylinder cases of uneven size batched in one launch per
+  stage, against one case per context in the mixed form and in both FP64
+  forms (the FP64 drop-in), with the batch's error against the exact form;
+* ``adjoint``: the discrete adjoint's cost ratio, J, dJ/dMs, dJ/dMA and
+  central differences;
+* ``output``: the stepping time with restart and Tecplot output every 100
+  steps, against none.
+
 Multi-GPU (torchrun): every rank runs an independent replica of the
 workload (the drop-in is single-GPU; the case does not shard), timing is the
 max over ranks and ``value`` is the total over ranks.
