@@ -12,8 +12,8 @@
 //      flux points (one thread per cell x family x line x variable);
 //   B1 physical flux at the interior flux points (thread per point);
 //   B2 Rusanov flux at the 4N face points of each cell (thread per point).
-//      The neighbour's trace at the face (9 contiguous values) comes from
-//      the trace buffer that the stage producing the input published.  Each
+//      The neighbour's trace at the face point comes from the trace buffer
+//      (trace_at) that the stage producing the input published.  Each
 //      shared face is evaluated by both of its cells, each with the
 //      reference's left/right assignment, so both get the value the
 //      reference scatters to them;
