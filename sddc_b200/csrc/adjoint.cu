@@ -37,6 +37,8 @@ namespace sddc {
 struct AdjWs {
     int grid = 0;            // VJP CTAs
     double *at = nullptr;    // adjoint traces, ncell * 4N * 12 (adj_trace_at)
+    double *at2 = nullptr;   // the next stage's, formed by the VJP epilogue
+    bool at_ready = false;   // at holds the current stage's traces already
     double *part = nullptr;  // [grid][8]
     AdjScalars *acc = nullptr;
     AdjRec *recs = nullptr;
@@ -54,7 +56,7 @@ void adjoint_free(sddc_ctx *ctx)
 {
     AdjWs *w = ctx->adj;
     if (!w) return;
-    void *b[] = {w->at, w->part, w->acc, w->recs, w->rec_n, w->lam, w->qbar, w->tq, w->wall};
+    void *b[] = {w->at, w->at2, w->part, w->acc, w->recs, w->rec_n, w->lam, w->qbar, w->tq, w->wall};
     for (void *p : b) cudaFree(p);
     if (w->host) cudaFreeHost(w->host);
     delete w;
@@ -111,6 +113,29 @@ cudaError_t launch_vjp(sddc_ctx *ctx, const VjpArgs &a)
     }
 }
 
+template <int N>
+cudaError_t launch_adj_reduce_n(sddc_ctx *ctx, int own_eig, int own_um, double dl, double du, double *out,
+                                const NextTraces &nt)
+{
+    AdjWs *w = ctx->adj;
+    adj_reduce_kernel<N><<<1, kRedThreads, 0, ctx->stream>>>(w->grid, w->part, w->acc, own_eig, own_um, dl, du, w->recs,
+                                                             w->rec_n, w->rec_n + 1, w->rec_cap, out, ctx->ops,
+                                                             ctx->err_flags, nt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_reduce(sddc_ctx *ctx, int own_eig, int own_um, double dl, double du, double *out,
+                              const NextTraces &nt)
+{
+    switch (ctx->N) {
+    case 2: return launch_adj_reduce_n<2>(ctx, own_eig, own_um, dl, du, out, nt);
+    case 3: return launch_adj_reduce_n<3>(ctx, own_eig, own_um, dl, du, out, nt);
+    case 4: return launch_adj_reduce_n<4>(ctx, own_eig, own_um, dl, du, out, nt);
+    case 5: return launch_adj_reduce_n<5>(ctx, own_eig, own_um, dl, du, out, nt);
+    default: return launch_adj_reduce_n<6>(ctx, own_eig, own_um, dl, du, out, nt);
+    }
+}
+
 Freestream ctx_fs(const sddc_ctx *ctx)
 {
     return Freestream{ctx->p.rinf, ctx->p.pinf, ctx->p.uinf, ctx->p.vinf, ctx->p.bxinf, ctx->p.byinf};
@@ -134,6 +159,7 @@ int ensure_ws(sddc_ctx *ctx)
     const size_t tr = nc * 4 * N * 9;
     int rc;
     if ((rc = alloc(ctx, (void **)&w->at, nc * 4 * N * 12 * sizeof(double), "adjoint traces")) ||
+        (rc = alloc(ctx, (void **)&w->at2, nc * 4 * N * 12 * sizeof(double), "adjoint traces")) ||
         (rc = alloc(ctx, (void **)&w->part, (size_t)w->grid * 8 * sizeof(double), "adjoint partials")) ||
         (rc = alloc(ctx, (void **)&w->acc, sizeof(AdjScalars), "adjoint scalars")) ||
         (rc = alloc(ctx, (void **)&w->recs, (size_t)w->rec_cap * sizeof(AdjRec), "argmax records")) ||
@@ -189,12 +215,17 @@ struct RevStage {
     double L = 0.0, U = 0.0, Lnext = 0.0, Unext = 0.0;  // maxima read by the stage and after it
     const double *cta_max = nullptr;  // the forward stage's per-CTA maxima
     bool reduce = true;
+    // the next reverse stage (whose output adjoint is out): its input state and
+    // c_k, for its adjoint traces in this stage's epilogue (null: not known yet)
+    const double *q_next = nullptr;
+    double scale_next = 0.0;
 };
 
 int reverse_stage(sddc_ctx *ctx, const RevStage &s)
 {
     AdjWs *w = ctx->adj;
-    if (s.xbar) CKA(launch_adj_trace(ctx, s.xbar, s.scale, s.q, w->at));
+    if (s.xbar && !w->at_ready) CKA(launch_adj_trace(ctx, s.xbar, s.scale, s.q, w->at));
+    double *at_next = s.q_next ? w->at2 : nullptr;
     const double c_h = std::sqrt(s.L * (s.L - s.U));
     VjpArgs a{};
     a.ncell = ctx->ncell;
@@ -227,7 +258,14 @@ int reverse_stage(sddc_ctx *ctx, const RevStage &s)
     for (int i = 0; i < kMaxN; i++) a.wq[i] = w->wq[i];
     a.part = w->part;
     a.err = ctx->err_flags;
+    a.q_next = s.q_next;
+    a.scale_next = s.scale_next;
+    a.at_next = at_next;
     CKA(launch_vjp(ctx, a));
+    // the traces formed for the next stage become the current ones (the
+    // reduction below corrects the cells its records change)
+    if (at_next) std::swap(w->at, w->at2);
+    w->at_ready = at_next != nullptr;
     const bool own_eig = s.reduce && s.Lnext > s.L, own_um = s.reduce && s.Unext > s.U;
     if (own_eig || own_um) {  // record where the stage raised a running maximum
         LocateArgs l{};
@@ -254,10 +292,8 @@ int reverse_stage(sddc_ctx *ctx, const RevStage &s)
         dl = (2.0 * s.L - s.U) / (2.0 * c_h);
         du = -s.L / (2.0 * c_h);
     }
-    adj_reduce_kernel<<<1, kRedThreads, 0, ctx->stream>>>(w->grid, w->part, w->acc, own_eig, own_um, dl, du, w->recs,
-                                                          w->rec_n, w->rec_n + 1, w->rec_cap, s.out, ctx->ops, ctx->N,
-                                                          ctx->err_flags);
-    CKA(cudaGetLastError());
+    const NextTraces nt{at_next, s.q_next, s.scale_next, ctx->met, ctx->p.vismode};
+    CKA(launch_adj_reduce(ctx, own_eig, own_um, dl, du, s.out, nt));
     return SDDC_OK;
 }
 
@@ -361,6 +397,7 @@ extern "C" int sddc_vjp_resid(sddc_ctx *ctx, const double *Rbar, double *Qbar, d
     CKA(cudaMemcpyAsync(w->host, ctx->maxima + 2 * ctx->slot, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CKA(cudaMemsetAsync(w->acc, 0, sizeof(AdjScalars), ctx->stream));
     CKA(cudaStreamSynchronize(ctx->stream));
+    w->at_ready = false;
     RevStage s;
     s.q = ctx->reg[0];
     s.t = w->tq;
@@ -480,6 +517,7 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
         // ---- reverse sweep ---------------------------------------------------------
         CKA(cudaMemsetAsync(w->acc, 0, sizeof(AdjScalars), ctx->stream));
         CKA(cudaMemsetAsync(w->rec_n, 0, 4 * sizeof(int), ctx->stream));
+        w->at_ready = false;
         double *Ab[6] = {A[0], A[1], A[2], A[3], A[4], A[5]};
         // the final state: dJ/dQ(n = nsteps)
         {
@@ -494,6 +532,8 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
             r.sx = in ? sx : 0.0;
             r.sy = in ? sy : 0.0;
             r.reduce = false;
+            r.q_next = S[5 * last - 1];  // stage 5 of the last step: input Q4
+            r.scale_next = B54 * o->dt;
             if ((rc = reverse_stage(ctx, r))) return rc;
         }
         for (int s = nseg - 1; s >= 0; s--) {
@@ -518,22 +558,26 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
                 RevStage r5;  // stage 5: input Q4 = S[i+4]
                 r5.q = S[i + 4]; r5.t = T[i + 4]; r5.xbar = Ab[5]; r5.scale = B54 * o->dt;
                 r5.ra = Ab[5]; r5.wa = A54; r5.out = Ab[4]; r5.wd = A52; r5.out2 = Ab[2];
+                r5.q_next = S[i + 3]; r5.scale_next = B43 * o->dt;
                 maxima(r5, 4);
                 if ((rc = reverse_stage(ctx, r5))) return rc;
                 RevStage r4;  // stage 4: input Q3 = S[i+3]
                 r4.q = S[i + 3]; r4.t = T[i + 3]; r4.xbar = Ab[4]; r4.scale = B43 * o->dt;
                 r4.ra = Ab[4]; r4.wa = A43; r4.out = Ab[3]; r4.wd = A40; r4.out2 = Ab[0];
+                r4.q_next = S[i + 2]; r4.scale_next = B32 * o->dt;
                 maxima(r4, 3);
                 if ((rc = reverse_stage(ctx, r4))) return rc;
                 RevStage r3;  // stage 3: input Q2 = S[i+2]
                 r3.q = S[i + 2]; r3.t = T[i + 2]; r3.xbar = Ab[3]; r3.scale = B32 * o->dt;
                 r3.ra = Ab[2]; r3.wa = 1.0; r3.rb = Ab[3]; r3.wb = A32; r3.out = Ab[2];
                 r3.rc = Ab[0]; r3.wc = 1.0; r3.wd = A30; r3.out2 = Ab[0];
+                r3.q_next = S[i + 1]; r3.scale_next = B21 * o->dt;
                 maxima(r3, 2);
                 if ((rc = reverse_stage(ctx, r3))) return rc;
                 RevStage r2;  // stage 2: input Q1 = S[i+1]
                 r2.q = S[i + 1]; r2.t = T[i + 1]; r2.xbar = Ab[2]; r2.scale = B21 * o->dt;
                 r2.ra = Ab[2]; r2.wa = 1.0; r2.out = Ab[1];
+                r2.q_next = S[i]; r2.scale_next = B10 * o->dt;
                 maxima(r2, 1);
                 if ((rc = reverse_stage(ctx, r2))) return rc;
                 RevStage r1;  // stage 1: input Q0 = S[i], the state after n steps
@@ -542,6 +586,10 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
                 const bool in = n >= o->n1 && n <= o->n2;
                 r1.sx = in ? sx : 0.0;
                 r1.sy = in ? sy : 0.0;
+                if (m > 0) {  // stage 5 of step n - 1 (its input is recomputed with the segment)
+                    r1.q_next = S[i - 1];
+                    r1.scale_next = B54 * o->dt;
+                }
                 maxima(r1, 0);
                 if ((rc = reverse_stage(ctx, r1))) return rc;
                 std::swap(Ab[0], Ab[5]);  // the adjoint of the state after n steps

@@ -77,16 +77,43 @@ struct VjpArgs {
     double wq[kMaxN];
     double *part;  // [8][CTAs]: cbar, pbar[6], 0
     unsigned *err;
+    // the next reverse stage's adjoint traces, formed from out (the adjoint of
+    // that stage's output) in the epilogue: its input state and lam_scale, and
+    // the trace buffer (null: its own trace launch forms them)
+    const double *q_next;
+    double scale_next;
+    double *at_next;
 };
 
 constexpr int kAdjCpb = 4;
 __host__ __device__ constexpr int adj_threads(int n, int cpb) { return (4 * n * cpb > 128 ? (4 * n * cpb + 31) / 32 * 32 : 128); }
 
+// Warps of vjp_kernel given to the face points (the rest take the interior
+// flux points): the count that minimises the slower side's rounds, with a
+// face point's Rusanov adjoint costing about kFaceCost interior points' flux
+// adjoints (measured on the B200 at N = 4); ties go to fewer face warps.
+constexpr int kFaceCost = 7;
+__host__ __device__ constexpr int adj_face_warps(int n, int cpb)
+{
+    const int nw = adj_threads(n, cpb) / 32, nf = cpb * 4 * n, ni = cpb * 2 * n * (n - 1);
+    int best = 1, cost = 1 << 30;
+    for (int w = 1; w < nw; w++) {
+        const int cf = (nf + 32 * w - 1) / (32 * w) * kFaceCost, ci = (ni + 32 * (nw - w) - 1) / (32 * (nw - w));
+        const int c = cf > ci ? cf : ci;
+        if (c < cost) {
+            cost = c;
+            best = w;
+        }
+    }
+    return best;
+}
+
 template <int N, int CPB> constexpr size_t vjp_smem_doubles()
 {
     constexpr int NQ = 9 * N * N, NP = N + 1, NN = N * N;
-    constexpr int kF = 2 * N * NP * 9, kV = 2 * N * NP * 2, kO = 4 * N * 9, NM = 2 * MetLayout<N>::kFam;
-    return (size_t)CPB * (2 * NQ + 2 * kF + kV + kO + MetLayout<N>::kJacPad + NN + NM) + 2 * NP * N + 8 * 32;
+    constexpr int kF = 2 * N * NP * 9, kV = 2 * N * NP * 2, kO = 4 * N * 9, kP = 4 * N * 13;
+    constexpr int NM = 2 * MetLayout<N>::kFam;
+    return (size_t)CPB * (2 * NQ + 2 * kF + kV + kO + kP + MetLayout<N>::kJacPad + NN + NM) + 2 * NP * N + 8 * 32;
 }
 
 // ---- adjoint traces ----------------------------------------------------------
@@ -114,7 +141,7 @@ __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, 
     constexpr int NQ = 9 * N * N, NN = N * N, CPB = kTraceCpb;
     __shared__ __align__(16) double sMu[CPB * NQ];  // lambda source, then -lambda/J
     __shared__ __align__(16) double sQs[CPB * NQ];  // the state
-    __shared__ double sB[CPB * NN];                 // Jac, then the divB adjoint over Jac
+    __shared__ double sB[CPB * NN];                 // Jac, 1/Jac, then the divB adjoint over Jac
     __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sAbort;
     const int tid = threadIdx.x, c0 = blockIdx.x * CPB, ncl = min(CPB, ncell - c0);
@@ -154,14 +181,16 @@ __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, 
         double db = 0.0;
         if (vismode == 1) {
             const double *qq = sQs + 9 * k;
-            const double ux = qq[1] / qq[0], uy = qq[2] / qq[0], uz = qq[3] / qq[0];
+            const double ri = 1.0 / qq[0], ux = qq[1] * ri, uy = qq[2] * ri, uz = qq[3] * ri;
             db = -lam_scale * (x[1] * qq[5] + x[2] * qq[6] + x[3] * qq[7] +
                                x[4] * ((ux * qq[5] + uy * qq[6]) + uz * qq[7]) + x[5] * ux + x[6] * uy + x[7] * uz);
         }
-        beta[it] = db / sB[k];
+        const double rJ = 1.0 / sB[k];
+        beta[it] = db * rJ;
+        sB[k] = rJ;
     }
     __syncthreads();
-    for (int k = tid; k < ncl * NQ; k += 128) sMu[k] = -(lam_scale * sMu[k]) / sB[k / 9];
+    for (int k = tid; k < ncl * NQ; k += 128) sMu[k] = -(lam_scale * sMu[k]) * sB[k / 9];
     __syncthreads();
     for (int k = tid, it = 0; k < ncl * NN; k += 128, it++) sB[k] = beta[it];
     __syncthreads();
@@ -188,6 +217,42 @@ __global__ void __launch_bounds__(128) adj_trace_kernel(int ncell, int vismode, 
         at[adj_trace_at<N>(c0 + c, lf, nfp - 1, 10)] = bs * nr[1];
         at[adj_trace_at<N>(c0 + c, lf, nfp - 1, 11)] = 0.0;
     }
+}
+
+// The adjoint trace at face point f (0..4N-1) of one cell from global memory,
+// in adj_trace_kernel's arithmetic: the reduction uses it to form again the
+// next stage's traces of the cells that its records changed.
+template <int N>
+__device__ void adj_trace_point(size_t cell, int f, const double *xbar, const double *q, double scale,
+                                const double *met, int vismode, const Ops &ops, double *at)
+{
+    using ML = MetLayout<N>;
+    constexpr int NQ = 9 * N * N;
+    const int nfp = 1 + f % N, lf = 1 + f / N;
+    int fam, line, r;
+    face_point<N>(lf, nfp, fam, line, r);
+    const double *mc = met + cell * ML::kSize;
+    double fb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, bs = 0.0;
+    for (int i = 0; i < N; i++) {
+        const int sp = fam == 0 ? i + N * line : line + N * i;
+        const double *x = xbar + cell * NQ + 9 * sp;
+        double db = 0.0;
+        if (vismode == 1) {
+            const double *qq = q + cell * NQ + 9 * sp;
+            const double ri = 1.0 / qq[0], ux = qq[1] * ri, uy = qq[2] * ri, uz = qq[3] * ri;
+            db = -scale * (x[1] * qq[5] + x[2] * qq[6] + x[3] * qq[7] + x[4] * ((ux * qq[5] + uy * qq[6]) + uz * qq[7]) +
+                           x[5] * ux + x[6] * uy + x[7] * uz);
+        }
+        const double rJ = 1.0 / mc[ML::kJac + sp];
+        const double m = ops.M[r * N + i];
+        for (int k = 0; k < 9; k++) fb[k] += m * (-(scale * x[k]) * rJ);
+        bs += m * (db * rJ);
+    }
+    const double *nr = mc + ML::normal(fam, line, r);
+    for (int k = 0; k < 9; k++) at[adj_trace_at<N>(cell, lf, nfp - 1, k)] = fb[k];
+    at[adj_trace_at<N>(cell, lf, nfp - 1, 9)] = bs * nr[0];
+    at[adj_trace_at<N>(cell, lf, nfp - 1, 10)] = bs * nr[1];
+    at[adj_trace_at<N>(cell, lf, nfp - 1, 11)] = 0.0;
 }
 
 // ---- running-max argmax records ----------------------------------------------------
@@ -252,7 +317,7 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     using ML = MetLayout<N>;
     constexpr int NT = adj_threads(N, CPB);
     constexpr int NQ = 9 * N * N, NP = N + 1, NN = N * N;
-    constexpr int kF = 2 * N * NP * 9, kV = 2 * N * NP * 2, kO = 4 * N * 9, NM = 2 * ML::kFam;
+    constexpr int kF = 2 * N * NP * 9, kV = 2 * N * NP * 2, kO = 4 * N * 9, kP = 4 * N * 13, NM = 2 * ML::kFam;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sQ = reinterpret_cast<double *>(smem_raw);  // [CPB][NQ] q, then qbar of the sources, then qbar
@@ -261,8 +326,11 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     double *sFb = sQf + CPB * kF;                       // [CPB][2][N][NP][9] flux adjoint, then state adjoint
     double *sVb = sFb + CPB * kF;                       // [CPB][2][N][NP][2] face-averaged Bx,By, then adjoint
     double *sQo = sVb + CPB * kV;                       // [CPB][4N][9] neighbour / ghost trace
+    // [CPB][4N][13] per face point: the partner's signed flux adjoint (9) and
+    // face-average adjoints (2), zero on boundary faces; the face's normal (2)
+    double *sPa = sQo + CPB * kO;
     constexpr int NJ = ML::kJacPad;
-    double *sJac = sQo + CPB * kO;                      // [CPB][NJ]
+    double *sJac = sPa + CPB * kP;                      // [CPB][NJ]
     double *sBeta = sJac + CPB * NJ;                    // [CPB][NN] adjoint of divB, over Jac
     double *sNrm = sBeta + CPB * NN;                    // [CPB][NM]
     double *sL = sNrm + CPB * NM;                       // [NP][N]
@@ -305,6 +373,30 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 if (xsrc) bulk_g2s(sA, xsrc, (unsigned)qbytes, &sBar);
             }
         }
+        // L2 prefetches of what later phases load from global memory: the RK
+        // registers of the epilogue, and per shared face the partner's trace
+        // and adjoint trace (each face's values are contiguous)
+        if (tid == 0) {
+            const size_t g0 = (size_t)c0 * NQ;
+            const double *regs[3] = {a.ra, a.rb, a.out2 ? a.rc : nullptr};
+            for (int m = 0; m < 3; m++)
+                if (regs[m] && (((uintptr_t)(regs[m] + g0) | qbytes) & 15) == 0)
+                    bulk_prefetch_l2(regs[m] + g0, (unsigned)qbytes);
+        } else if (tid >= 32 && tid < 32 + ncl * 4) {
+            const int c = (tid - 32) >> 2, lf = 1 + ((tid - 32) & 3);
+            const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
+            const int kind = rec.y & 0xff;
+            if (kind == kFaceLeft || kind == kFaceRight) {
+                const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
+                // the face's 9N trace values, widened to 16-byte bounds (the
+                // buffer, 288N bytes per cell, starts and ends on one)
+                const uintptr_t t0 = (uintptr_t)(a.t_in + trace_at<N>(pc, plf, 0, 0)) & ~(uintptr_t)15;
+                const uintptr_t t1 = ((uintptr_t)(a.t_in + trace_at<N>(pc, plf, 0, 9)) + 15) & ~(uintptr_t)15;
+                if (((uintptr_t)a.t_in & 15) == 0) bulk_prefetch_l2((const void *)t0, (unsigned)(t1 - t0));
+                if (a.xbar && ((uintptr_t)a.at & 15) == 0)
+                    bulk_prefetch_l2(a.at + adj_trace_at<N>(pc, plf, 0, 0), 12 * N * sizeof(double));
+            }
+        }
         for (int k = tid; k < NP * N; k += NT) {
             sL[k] = ops.L[k];
             sM[k] = ops.M[k];
@@ -329,15 +421,18 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     }
     __syncthreads();
     if (sAbort) return;
+    // lambda (first read two barriers on); the packed metric records, staged in
+    // sQf, are converted before phase A overwrites sQf
     for (int k = tid; k < ncl * NQ; k += NT) sA[k] = a.xbar ? a.lam_scale * sA[k] : 0.0;
-    if (!split)
+    if (!split) {
         for (int k = tid; k < ncl * ML::kSize; k += NT) {
             const int c = k / ML::kSize, o = k - c * ML::kSize;
             const double v = sQf[k];
             if (o < NM) sNrm[c * NM + o] = v;
             else if (o < NM + NN) sJac[c * NJ + (o - NM)] = v;
         }
-    __syncthreads();
+        __syncthreads();
+    }
 
     // ---- primal: flux-point states (phase A of the stage kernel) ----------------
     for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
@@ -357,16 +452,50 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     }
     __syncthreads();
 
-    // ---- primal: neighbour / ghost traces and face-averaged Bx, By -------------------
-    for (int t = tid; t < ncl * 4 * N; t += NT) {
+    // ---- primal: neighbour / ghost traces and face-averaged Bx, By; on the ---------
+    // ---- other threads the partner's adjoint trace and the face normal -------------
+    for (int t2 = tid; t2 < 2 * ncl * 4 * N; t2 += NT) {
+        const bool part = t2 >= ncl * 4 * N;
+        const int t = part ? t2 - ncl * 4 * N : t2;
         const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
         int fam, line, r;
         face_point<N>(lf, nfp, fam, line, r);
-        const double *own = sQf + c * kF + ((fam * N + line) * NP + r) * 9;
-        double oth[9];
         const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
         const int kind = rec.y & 0xff;
         const bool own_right = kind == kFaceRight;
+        if (part) {
+            const double *onrm = sNrm + c * NM + ML::normal(fam, line, r);
+            double v[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, onrm[0], onrm[1]};
+            if (kind == kFaceLeft || own_right) {
+                const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
+                int pfam, pline, pr;
+                face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
+                if (own_right) {  // the flux is formed with the left (partner) cell's normal
+                    const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
+                    v[11] = __ldg(pn);
+                    v[12] = __ldg(pn + 1);
+                }
+                // the partner's slot enters with sign_l * sign_r unless it is
+                // the left cell's
+                const int sign_l = own_right ? (pr == 0 ? -1 : 1) : (r == 0 ? -1 : 1);
+                const int sign_r = own_right ? (r == N ? -1 : 1) : (pr == N ? -1 : 1);
+                const double ps = own_right ? 1.0 : (double)(sign_l * sign_r);
+                if (a.xbar) {
+#pragma unroll
+                    for (int k = 0; k < 9; k++) v[k] = ps * a.at[adj_trace_at<N>(pc, plf, N - nfp, k)];
+                    if (a.vismode == 1) {
+                        v[9] = a.at[adj_trace_at<N>(pc, plf, N - nfp, 9)];
+                        v[10] = a.at[adj_trace_at<N>(pc, plf, N - nfp, 10)];
+                    }
+                }
+            }
+            double *pa = sPa + c * kP + (t % (4 * N)) * 13;
+#pragma unroll
+            for (int k = 0; k < 13; k++) pa[k] = v[k];
+            continue;
+        }
+        const double *own = sQf + c * kF + ((fam * N + line) * NP + r) * 9;
+        double oth[9];
         if (kind == kFaceLeft || own_right) {
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
 #pragma unroll
@@ -388,7 +517,7 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     // ---- per solution point: divB, the source adjoint, -lambda/J, divB adjoint ------
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
-        const double J = sJac[c * NJ + i + N * j];
+        const double rJ = 1.0 / sJac[c * NJ + i + N * j];
         const double *met = sNrm + c * NM;
         double divB = 0.0;
         if (a.vismode == 1) {
@@ -405,11 +534,11 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 ay += V(0, j, r, 1) * sM[r * N + i] * met[ML::normal(0, j, r) + 1];
                 by += V(1, i, r, 1) * sM[r * N + j] * met[ML::normal(1, i, r) + 1];
             }
-            divB = (ax + bx) / J + (ay + by) / J;
+            divB = ((ax + bx) + (ay + by)) * rJ;
         }
         double *qs = sQ + c * NQ + 9 * (i + N * j);
         double *lam = sA + c * NQ + 9 * (i + N * j);
-        const double rho = qs[0], ux = qs[1] / rho, uy = qs[2] / rho, uz = qs[3] / rho;
+        const double rho = qs[0], ri = 1.0 / rho, ux = qs[1] * ri, uy = qs[2] * ri, uz = qs[3] * ri;
         const double Bx = qs[5], By = qs[6], Bz = qs[7];
         double db = 0.0;
         if (a.vismode == 1)
@@ -420,10 +549,10 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
         const double vb = -divB * (lam[4] * By + lam[6]);
         const double wb = -divB * (lam[4] * Bz + lam[7]);
         double src[9];
-        src[0] = -(ub * ux + vb * uy + wb * uz) / rho;
-        src[1] = ub / rho;
-        src[2] = vb / rho;
-        src[3] = wb / rho;
+        src[0] = -(ub * ux + vb * uy + wb * uz) * ri;
+        src[1] = ub * ri;
+        src[2] = vb * ri;
+        src[3] = wb * ri;
         src[4] = 0.0;
         src[5] = -divB * (lam[1] + lam[4] * ux);
         src[6] = -divB * (lam[2] + lam[4] * uy);
@@ -432,9 +561,9 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
 #pragma unroll
         for (int k = 0; k < 9; k++) {
             qs[k] = src[k];
-            lam[k] = -lam[k] / J;
+            lam[k] = -lam[k] * rJ;
         }
-        sBeta[c * NN + i + N * j] = db / J;
+        sBeta[c * NN + i + N * j] = db * rJ;
     }
     __syncthreads();
 
@@ -464,10 +593,10 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
 
     double cbar = 0.0, pb[6] = {0, 0, 0, 0, 0, 0};
     // The point adjoints: face points on the first kFaceWarps warps, interior
-    // flux points on the others, in the ratio of their cost (a face point's
-    // Rusanov adjoint costs about twice an interior point's flux adjoint).
-    constexpr int NW = NT / 32;
-    constexpr int kFaceWarps = (NW * 4 + (N + 3) / 2) / (N + 3) < 1 ? 1 : (NW * 4 + (N + 3) / 2) / (N + 3);
+    // flux points on the others (adj_face_warps balances their rounds).  The
+    // interior warps then add the interior flux points' share of the
+    // transposed interpolation while the face warps finish.
+    constexpr int kFaceWarps = adj_face_warps(N, CPB);
     const int wid = tid >> 5;
     if (wid >= kFaceWarps) {
         // ---- interior flux points ---------------------------------------------------
@@ -488,6 +617,17 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
 #pragma unroll
             for (int k = 0; k < 9; k++) fb[k] = qb[k];
         }
+        // the interior warps' own barrier: their flux-point adjoints are all in
+        asm volatile("bar.sync 1, %0;" ::"r"(nth) : "memory");
+        for (int t = me; t < ncl * NQ; t += nth) {
+            const int v = t % 9, i = (t / 9) % N, j = (t / (9 * N)) % N, c = t / NQ;
+            const double *gx = sFb + c * kF + (0 * N + j) * NP * 9 + v;  // xi-line j
+            const double *gy = sFb + c * kF + (1 * N + i) * NP * 9 + v;  // eta-line i
+            double acc = sQ[t];
+#pragma unroll
+            for (int r = 1; r < N; r++) acc += sL[r * N + i] * gx[r * 9] + sL[r * N + j] * gy[r * 9];
+            sQ[t] = acc;
+        }
     } else {
         // ---- face points ------------------------------------------------------------
         for (int t = tid; t < ncl * 4 * N; t += 32 * kFaceWarps) {
@@ -502,8 +642,8 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
             const int kind = rec.y & 0xff;
             const bool pair = kind == kFaceLeft || kind == kFaceRight;
             const bool own_right = kind == kFaceRight;
-            const double *onrm = sNrm + c * NM + ML::normal(fam, line, r);
-            double n0, n1;
+            const double *pa = sPa + c * kP + (t % (4 * N)) * 13;
+            const double n0 = pa[11], n1 = pa[12];
             int sign_l, sign_r;
             double fbar[9], vbx = 0.0, vby = 0.0;
             if (a.vismode == 1) {
@@ -511,34 +651,20 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 vby = sVb[c * kV + slot * 2 + 1];
             }
             if (pair) {
-                const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
+                const int plf = (rec.y >> 8) & 0xff;
                 int pfam, pline, pr;
                 face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
-                if (!own_right) {
-                    n0 = onrm[0]; n1 = onrm[1];
-                    sign_l = r == 0 ? -1 : 1;
-                    sign_r = pr == N ? -1 : 1;
-                } else {
-                    const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
-                    n0 = __ldg(pn);
-                    n1 = __ldg(pn + 1);
-                    sign_l = pr == 0 ? -1 : 1;
-                    sign_r = r == N ? -1 : 1;
-                }
-                const double slr = (double)(sign_l * sign_r);
-                const double ms = own_right ? slr : 1.0, ps = own_right ? 1.0 : slr;
+                sign_l = own_right ? (pr == 0 ? -1 : 1) : (r == 0 ? -1 : 1);
+                sign_r = own_right ? (r == N ? -1 : 1) : (pr == N ? -1 : 1);
+                const double ms = own_right ? (double)(sign_l * sign_r) : 1.0;
+                // the partner's share (staged signed, zero without xbar)
 #pragma unroll
-                for (int k = 0; k < 9; k++) fbar[k] = ms * fown[k];
-                if (a.xbar) {
-#pragma unroll
-                    for (int k = 0; k < 9; k++) fbar[k] += ps * a.at[adj_trace_at<N>(pc, plf, N - nfp, k)];
-                    if (a.vismode == 1) {
-                        vbx += a.at[adj_trace_at<N>(pc, plf, N - nfp, 9)];
-                        vby += a.at[adj_trace_at<N>(pc, plf, N - nfp, 10)];
-                    }
+                for (int k = 0; k < 9; k++) fbar[k] = ms * fown[k] + pa[k];
+                if (a.vismode == 1) {
+                    vbx += pa[9];
+                    vby += pa[10];
                 }
             } else {
-                n0 = onrm[0]; n1 = onrm[1];
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = 1;
 #pragma unroll
@@ -550,22 +676,24 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 }
             }
             const double *ql = own_right ? oth : own, *qr = own_right ? own : oth;
-            // this cell's share of the c_h adjoint: its own flux slot
-            cbar += (own_right ? (double)(sign_l * sign_r) : 1.0) * rusanov_wdfdc(ql, qr, n0, n1, sign_l, fown);
             double qown[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, eig, um;
             // the face-averaged Bx, By feed the gradients of both cells
             qown[5] = 0.5 * vbx;
             qown[6] = 0.5 * vby;
+            // this cell's share of the c_h adjoint comes from its own flux
+            // slot (fown, weighted by the slot's sign)
+            double wdc;
             if (pair) {
-                rusanov_vjp(ql, qr, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, own_right ? nullptr : qown,
-                            own_right ? qown : nullptr, eig, um);
+                wdc = rusanov_vjp(ql, qr, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, own_right ? nullptr : qown,
+                                  own_right ? qown : nullptr, eig, um, nullptr, fown);
             } else {
                 double qgb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                 qgb[5] = 0.5 * vbx;
                 qgb[6] = 0.5 * vby;
-                rusanov_vjp(own, oth, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, qown, qgb, eig, um);
+                wdc = rusanov_vjp(own, oth, n0, n1, sign_l, a.c_h, fbar, 0.0, 0.0, qown, qgb, eig, um, nullptr, fown);
                 bc_ghost_vjp(kind, own, n0, n1, a.vismode, a.fs, qgb, qown, pb);
             }
+            cbar += (own_right ? (double)(sign_l * sign_r) : 1.0) * wdc;
 
 #pragma unroll
             for (int k = 0; k < 9; k++) fown[k] = qown[k];
@@ -573,15 +701,26 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
     }
     __syncthreads();
 
-    // ---- transposed interpolation: state adjoint at the solution points -------------
+    // the next stage's input state, for its adjoint traces, by a bulk copy into
+    // sQf (no longer read) that lands during the steps below
+    const bool fuse = a.at_next != nullptr;  // uniform
+    const double *qn = fuse ? a.q_next + (size_t)c0 * NQ : nullptr;
+    const bool qn_bulk = fuse && (((uintptr_t)qn | ((size_t)ncl * NQ * sizeof(double))) & 15) == 0;
+    __shared__ __align__(8) unsigned long long sBarN;
+    if (qn_bulk && tid == 0) {
+        fence_proxy_async();
+        mbar_init(&sBarN, 1);
+        mbar_expect_tx(&sBarN, (unsigned)(ncl * NQ * sizeof(double)));
+        bulk_g2s(sQf, qn, (unsigned)(ncl * NQ * sizeof(double)), &sBarN);
+    }
+
+    // ---- transposed interpolation, the face points' share (the interior flux ---------
+    // ---- points' share is in): state adjoint at the solution points ------------------
     for (int t = tid; t < ncl * NQ; t += NT) {
         const int v = t % 9, i = (t / 9) % N, j = (t / (9 * N)) % N, c = t / NQ;
         const double *gx = sFb + c * kF + (0 * N + j) * NP * 9 + v;  // xi-line j
         const double *gy = sFb + c * kF + (1 * N + i) * NP * 9 + v;  // eta-line i
-        double acc = sQ[t];
-#pragma unroll
-        for (int r = 0; r < NP; r++) acc += sL[r * N + i] * gx[r * 9] + sL[r * N + j] * gy[r * 9];
-        sQ[t] = acc;
+        sQ[t] += (sL[i] * gx[0] + sL[j] * gy[0]) + (sL[N * N + i] * gx[N * 9] + sL[N * N + j] * gy[N * 9]);
     }
     __syncthreads();
 
@@ -611,9 +750,65 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
                 double o = 0.0;
                 if (a.ra) o = a.wa * va[u];
                 if (a.rb) o = o + a.wb * vb[u];
-                a.out[g] = o + sQ[e];
+                const double ov = o + sQ[e];
+                a.out[g] = ov;
+                if (fuse) sQ[e] = ov;
                 if (a.out2) a.out2[g] = (a.rc ? a.wc * vc[u] : 0.0) + a.wd * vx[u];
             }
+        }
+    }
+
+    // ---- the next reverse stage's adjoint traces from out (adj_trace_kernel's ----------
+    // ---- arithmetic): -lambda/J and the divB adjoint per point, then per face point -----
+    if (fuse) {
+        if (!qn_bulk)
+            for (int k = tid; k < ncl * NQ; k += NT) sQf[k] = qn[k];
+        else if (tid == 0 && !mbar_wait_bounded(&sBarN, 0)) {
+            atomicOr(a.err, kErrStagingTimeout);  // the copy did not complete
+            sAbort = 1;
+            mbar_wait_bounded(&sBarN, 0);
+        }
+        __syncthreads();
+        if (sAbort) return;
+        for (int k = tid; k < ncl * NN; k += NT) {
+            double *x = sQ + 9 * k;
+            double db = 0.0;
+            if (a.vismode == 1) {
+                const double *qq = sQf + 9 * k;
+                const double ri = 1.0 / qq[0], ux = qq[1] * ri, uy = qq[2] * ri, uz = qq[3] * ri;
+                db = -a.scale_next * (x[1] * qq[5] + x[2] * qq[6] + x[3] * qq[7] +
+                                      x[4] * ((ux * qq[5] + uy * qq[6]) + uz * qq[7]) + x[5] * ux + x[6] * uy +
+                                      x[7] * uz);
+            }
+            const int c = k / NN;
+            const double rJ = 1.0 / sJac[c * NJ + (k - c * NN)];
+            sBeta[k] = db * rJ;
+#pragma unroll
+            for (int m = 0; m < 9; m++) x[m] = -(a.scale_next * x[m]) * rJ;
+        }
+        __syncthreads();
+        for (int t = tid; t < ncl * 4 * N; t += NT) {
+            const int c = t / (4 * N), f = t - c * 4 * N;
+            const int nfp = 1 + f % N, lf = 1 + f / N;
+            int fam, line, r;
+            face_point<N>(lf, nfp, fam, line, r);
+            double fb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, bs = 0.0;
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                const int sp = fam == 0 ? i + N * line : line + N * i;
+                const double m = sM[r * N + i];
+                const double *mu = sQ + c * NQ + 9 * sp;
+#pragma unroll
+                for (int k = 0; k < 9; k++) fb[k] += m * mu[k];
+                bs += m * sBeta[c * NN + sp];
+            }
+            const double *nr = sNrm + c * NM + ML::normal(fam, line, r);
+            double *o = a.at_next;
+#pragma unroll
+            for (int k = 0; k < 9; k++) o[adj_trace_at<N>(c0 + c, lf, nfp - 1, k)] = fb[k];
+            o[adj_trace_at<N>(c0 + c, lf, nfp - 1, 9)] = bs * nr[0];
+            o[adj_trace_at<N>(c0 + c, lf, nfp - 1, 10)] = bs * nr[1];
+            o[adj_trace_at<N>(c0 + c, lf, nfp - 1, 11)] = 0.0;
         }
     }
 
@@ -642,13 +837,23 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
 // equally among the points attaining the maximum, a shared face counted
 // once); then restarts the accumulation at this stage's owner and adds this
 // stage's c_h adjoint (dc/dL, dc/dU from the maxima it read).
+// Where the VJP formed the next stage's adjoint traces from out, the cells
+// that the records change get theirs formed again (next.at non-null).
 constexpr int kRedThreads = 1024;
+struct NextTraces {
+    double *at;       // the next stage's adjoint traces (null: none formed yet)
+    const double *q;  // its input state
+    double scale;     // its lam_scale
+    const double *met;
+    int vismode;
+};
+template <int N>
 static __global__ void __launch_bounds__(kRedThreads) adj_reduce_kernel(int nblk, const double *__restrict__ part,
                                                                  AdjScalars *acc, int owner_eig, int owner_um,
                                                                  double dc_dl, double dc_du,
                                                                  const AdjRec *__restrict__ recs, int *rec_n,
                                                                  int *rec_cnt, int rec_cap, double *out,
-                                                                 const Ops ops, int N, unsigned *err)
+                                                                 const Ops ops, unsigned *err, NextTraces next)
 {
     __shared__ double s[7][kRedThreads / 32];
     __shared__ double w[2];
@@ -688,6 +893,13 @@ static __global__ void __launch_bounds__(kRedThreads) adj_reduce_kernel(int nblk
             if (R.p[m] != 0.0) atomicAdd(&ps[m], wt * R.p[m]);
     }
     __syncthreads();
+    if (next.at)  // one warp per record, a lane per face point of its cell
+        for (int k = wid; k < nrec; k += kRedThreads / 32) {
+            const AdjRec &R = recs[k];
+            if (w[R.kind] == 0.0) continue;
+            for (int f = lane; f < 4 * N; f += 32)
+                adj_trace_point<N>((size_t)R.cell, f, out, next.q, next.scale, next.met, next.vismode, ops, next.at);
+        }
     if (tid == 0) {
         double t[7] = {0, 0, 0, 0, 0, 0, 0};
         for (int x = 0; x < kRedThreads / 32; x++)

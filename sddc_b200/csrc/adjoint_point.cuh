@@ -25,6 +25,17 @@ constexpr double kG1 = kGam - 1.0;
 
 SDDC_HD double sgn1(double x) { return x < 0.0 ? -1.0 : 1.0; }
 
+// 1/sqrt(x): the device's reciprocal square root (within an ulp or so, which
+// the adjoint's tolerance allows); the host's sqrt and divide
+SDDC_HD double Rsqrt(double x)
+{
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+
 // Adjoint of Fc = n0*F(Q, c) + n1*G(Q, c) at one interior flux point.
 // fb: adjoint of Fc; qb += (dFc/dQ)^T fb.  Returns fb . dFc/dc; um gets the
 // point's velocity maximum max(|u|, |v|, |w|) and um_d its gradient with
@@ -181,13 +192,15 @@ SDDC_HD void rus_side_vjp(const RusSide &s, double c, double ux, double uy, cons
 // fb: adjoint of f; eb0, umb0: extra adjoints of the wave speed and of the
 // face velocity maximum.  qlb, qrb accumulate; either may be null (that
 // side's adjoint is not formed).  eig and um return the wave speed and
-// velocity maximum; dfdc (nullable) gets d f / d c_h.
-SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double c,
-                         const double *fb, double eb0, double umb0, double *qlb, double *qrb, double &eig, double &um,
-                         double *dfdc = nullptr)
+// velocity maximum; dfdc (nullable) gets d f / d c_h.  Returns
+// wc . d f / d c_h (0 when wc is null).
+SDDC_HD double rusanov_vjp(const double *Ql, const double *Qr, double n0, double n1, int sign_l, double c,
+                           const double *fb, double eb0, double umb0, double *qlb, double *qrb, double &eig,
+                           double &um, double *dfdc = nullptr, const double *wc = nullptr)
 {
-    const double magnorm = Sqrt(n0 * n0 + n1 * n1);
-    const double sm = (double)sign_l / magnorm;
+    const double n2 = n0 * n0 + n1 * n1, rm = Rsqrt(n2);
+    const double magnorm = n2 * rm;
+    const double sm = (double)sign_l * rm;
     const double ux = n0 * sm, uy = n1 * sm;
     // the quantities both sides share
     double Vn_s, pg[2], rho[2], Bh[3], uvw[3], Bn[2];
@@ -216,14 +229,23 @@ SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n
         dfdc[6] = K * ps * uy;
         dfdc[8] = K * (Bn[0] + Bn[1]);
     }
+    const double wdc = wc ? K * (wc[4] * (Ql[8] * Bn[0] + Qr[8] * Bn[1]) + (wc[5] * ux + wc[6] * uy) * (Ql[8] + Qr[8]) +
+                                 wc[8] * (Bn[0] + Bn[1]))
+                          : 0.0;
     const double bn = Bh[0] * ux + Bh[1] * uy;
     const double S = rho[0] + rho[1], iS = 1.0 / S;
     const double ca = kGam * (pg[0] + pg[1]) * iS;
     const double cd = 2.0 * ((Bh[0] * Bh[0] + Bh[1] * Bh[1]) + Bh[2] * Bh[2]) * iS;
     const double cn = 2.0 * bn * bn * iS;
     const double cad = ca + cd;
-    const double ct = Sqrt(cad * cad - 4.0 * ca * cn);
-    const double cf = Sqrt(0.5 * (cad + ct));
+    // ct = sqrt(disc) and cf = sqrt(xf) through their reciprocal square
+    // roots, which the adjoint needs as well (ct's slope is taken as 0 at
+    // disc = 0)
+    const double disc = cad * cad - 4.0 * ca * cn;
+    const double rct = disc > 0.0 ? Rsqrt(disc) : 0.0;
+    const double ct = disc > 0.0 ? disc * rct : Sqrt(disc);
+    const double xf = 0.5 * (cad + ct), rcf = Rsqrt(xf);
+    const double cf = xf * rcf;
     eig = 0.5 * Abs(Vn_s) + cf;
     const double xu = 0.5 * Abs(uvw[0]), xv = 0.5 * Abs(uvw[1]), xw = 0.5 * Abs(uvw[2]);
     const double m1 = Max(xu, xv);
@@ -235,8 +257,8 @@ SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n
     for (int k = 0; k < 9; k++) ebar -= K * fb[k] * (Qr[k] - Ql[k]);
     // eig = |Vnl + Vnr| / 2 + cf
     const double Vnb = 0.5 * sgn1(Vn_s) * ebar;
-    const double q4 = 0.25 * ebar / cf;  // d eig / d cad = d eig / d ct
-    const double Db = ct > 0.0 ? 0.5 * q4 / ct : 0.0;
+    const double q4 = 0.25 * ebar * rcf;  // d eig / d cad = d eig / d ct
+    const double Db = 0.5 * q4 * rct;
     const double cadb = q4 + 2.0 * cad * Db;
     const double cab = -4.0 * cn * Db + cadb;
     const double cnb = -4.0 * ca * Db;
@@ -261,6 +283,7 @@ SDDC_HD void rusanov_vjp(const double *Ql, const double *Qr, double n0, double n
         rus_side(Q, ux, uy, Sd);
         rus_side_vjp(Sd, c, ux, uy, g, Vnb, pgb, Bhalf, Sb, uvwb, qb);
     }
+    return wdc;
 }
 
 // w . d f / d c_h of the Rusanov flux (f's c_h terms: k = 4, 5, 6, 8)

@@ -180,6 +180,12 @@ __device__ __forceinline__ void bulk_s2g(void *dst, const void *src, unsigned by
 }
 // the issuing thread's bulk stores have read their shared-memory source
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// a hint that brings [src, src + bytes) into L2; src 16-byte aligned, bytes a
+// multiple of 16, the range inside one allocation
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 
 template <int N, typename R, bool DIAG> struct Smem {
     static constexpr int NQ = 9 * N * N;

@@ -95,7 +95,7 @@ int main()
             double fwd = eb0 * eig.d[0] + umb0 * um.d[0], scale = std::fabs(eb0 * eig.d[0]) + std::fabs(umb0 * um.d[0]);
             for (int k = 0; k < 9; k++) { fwd += fb[k] * Fl[k].d[0]; scale += std::fabs(fb[k] * Fl[k].d[0]); }
             double qlb[9] = {0}, qrb[9] = {0}, eigv, umv, dfdc[9];
-            rusanov_vjp(ql, qr, n0, n1, sl, c, fb, eb0, umb0, qlb, qrb, eigv, umv, dfdc);
+            const double wdc = rusanov_vjp(ql, qr, n0, n1, sl, c, fb, eb0, umb0, qlb, qrb, eigv, umv, dfdc, fb);
             double rev = 0.0;
             for (int k = 0; k < 9; k++) rev += qlb[k] * vl[k] + qrb[k] * vr[k];
             report("rusanov <w,Jv>", fwd, rev, scale);
@@ -119,6 +119,7 @@ int main()
                 ws += std::fabs(fb[k] * Fl[k].d[0]);
             }
             report("rusanov w.dfdc", wd, rusanov_wdfdc(ql, qr, n0, n1, sl, fb), ws + 1.0);
+            report("rusanov w.dfdc (returned)", wd, wdc, ws + 1.0);
         }
         // ---- boundary ghost states --------------------------------------------
         {
