@@ -9,17 +9,22 @@
 // adjoint_point.cuh.  The AV sensor enters no residual (its coefficients are
 // zero, getrusanov.f90:326,328) and so has no adjoint.
 //
-// Two launches per reverse stage:
-//   adj_trace_kernel  per (cell, face point): the adjoint of the flux value
+// Per reverse stage:
+//   adjoint traces    per (cell, face point): the adjoint of the flux value
 //                     and of the face-averaged Bx, By that this cell's
 //                     residual sees at the face point (its neighbour needs
 //                     them: a shared face's flux and average enter both
-//                     cells' residuals);
+//                     cells' residuals).  They depend on the cell's own
+//                     output adjoint only, which is the previous reverse
+//                     stage's out: that stage's vjp_kernel forms them in its
+//                     epilogue when it knows this stage's input state, else
+//                     adj_trace_kernel does;
 //   vjp_kernel        per tile of cells, staged in shared memory: primal
 //                     recomputation (traces, divB), the transposed
 //                     divergence and gradient, the point adjoints, the
-//                     transposed interpolation, and the RK reverse update as
-//                     an element-wise epilogue.
+//                     transposed interpolation, the RK reverse update as an
+//                     element-wise epilogue, and the next stage's adjoint
+//                     traces.
 // c_h = sqrt(L (L - U)) is a function of the running maxima L, U of the wave
 // speed and velocity over all earlier stages; its adjoint is carried by
 // adj_reduce_kernel to the stage and points where the maximum was attained
