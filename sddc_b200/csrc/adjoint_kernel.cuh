@@ -121,6 +121,13 @@ template <int N, int CPB> constexpr size_t vjp_smem_doubles()
     return (size_t)CPB * (2 * NQ + 2 * kF + kV + kO + kP + MetLayout<N>::kJacPad + NN + NM) + 2 * NP * N + 8 * 32;
 }
 
+// the tile fits a CTA's shared memory (227 KB) at every N; at N = 4 four
+// CTAs fit an SM (228 KB, 1 KB reserved per CTA), which the 128-register cap
+// of vjp_kernel's launch bounds assumes
+static_assert(vjp_smem_doubles<6, kAdjCpb>() * sizeof(double) <= 227 * 1024, "VJP tile exceeds shared memory");
+static_assert(4 * (vjp_smem_doubles<4, kAdjCpb>() * sizeof(double) + 1024) <= 228 * 1024,
+              "VJP tile at N = 4 no longer fits four CTAs per SM");
+
 // ---- adjoint traces ----------------------------------------------------------
 // at(cell, lf, nfp) = (Fbar(9), Vbar_Bx, Vbar_By, 0): the adjoint of this
 // cell's flux value at the face point (from the divergence, compresid.f90:
