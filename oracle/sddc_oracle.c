@@ -39,6 +39,21 @@ typedef orc_real real;
 static inline real r_sqrt(real x) { return csqrt(x); }
 static inline real r_abs(real x) { return creal(x) < 0.0 ? -x : x; }
 static inline real r_max(real a, real b) { return creal(b) > creal(a) ? b : a; }
+#elif defined(ORC_COUNT)
+/* the operation-count build (C++): |x| and max() select, they count nothing */
+orc_tally_t orc_tally;
+#define RV(x) ((x).v)
+static inline real r_sqrt(real x) { return orc_count_sqrt(x); }
+static inline real r_abs(real x) { return x.v < 0.0 ? -x : x; }
+static inline real r_max(real a, real b) { return b.v > a.v ? b : a; }
+extern "C" void orc_count_read(unsigned long long *out, int reset)
+{
+    out[0] = orc_tally.add;
+    out[1] = orc_tally.mul;
+    out[2] = orc_tally.div;
+    out[3] = orc_tally.sqrt;
+    if (reset) orc_tally = orc_tally_t{0, 0, 0, 0};
+}
 #else
 #define RV(x) (x)
 #define r_sqrt sqrt
@@ -276,7 +291,16 @@ void orc_set_threads(int n)
 
 int orc_get_threads(void) { return g_threads; }
 
+#ifdef ORC_COUNT
+/* C++ converts void * to a typed pointer only explicitly */
+struct orc_anyptr {
+    void *p;
+    template <class T> operator T *() const { return static_cast<T *>(p); }
+};
+static orc_anyptr zalloc(size_t n) { return orc_anyptr{calloc(n ? n : 1, 1)}; }
+#else
 static void *zalloc(size_t n) { return calloc(n ? n : 1, 1); }
+#endif
 
 orc_ctx *orc_create(const orc_params *p)
 {

@@ -27,10 +27,21 @@ typedef struct orc_ctx orc_ctx;
 
 /* State arithmetic: double, or double _Complex in the complex-step tangent
    build (libsddc_oracle_cs.so, -DORC_CSTEP), whose state arrays are
-   interleaved (re, im) pairs. */
+   interleaved (re, im) pairs, or a double that counts its operations in the
+   operation-count build (libsddc_oracle_count.so, C++, -DORC_COUNT), whose
+   arrays are plain doubles. */
 #ifdef ORC_CSTEP
 #include <complex.h>
 typedef double _Complex orc_real;
+#elif defined(ORC_COUNT)
+#ifdef __cplusplus
+}
+#endif
+#include "orc_count.hpp"
+#ifdef __cplusplus
+extern "C" {
+#endif
+typedef orc_count orc_real;
 #else
 typedef double orc_real;
 #endif

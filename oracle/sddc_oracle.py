@@ -10,6 +10,11 @@ pinned by the known-answer tests in tests/test_oracle_kat.py.
 (libsddc_oracle_cs.so): its state arrays are complex128, and a state
 Q + 1j*h*V evaluated with h ~ 1e-30 carries the FP64 tangent dR/dQ . V in
 its imaginary part divided by h.
+
+``Oracle(..., count=True)`` loads the operation-count build
+(libsddc_oracle_count.so, the same source as C++ with a counting double):
+``op_counts()`` returns the +/-, *, / and square roots applied to
+state-dependent quantities since the last reset.
 """
 from __future__ import annotations
 
@@ -22,6 +27,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libsddc_oracle.so")
 LIB_CS = os.path.join(HERE, "libsddc_oracle_cs.so")
+LIB_COUNT = os.path.join(HERE, "libsddc_oracle_count.so")
 
 _I = ctypes.c_int
 _L = ctypes.c_long
@@ -44,7 +50,7 @@ def build() -> str:
     return LIB
 
 
-def _load(path, tangent):
+def _load(path, tangent, count=False):
     if not os.path.exists(path):
         build()
     L = ctypes.CDLL(path)
@@ -66,6 +72,9 @@ def _load(path, tangent):
     L.orc_setsandpoints.argtypes = [_I, _PD, _PD]
     L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
     L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
+    if count:  # the operation-count build: the residual path only
+        L.orc_count_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), _I]
+        return L
     if not tangent:  # complex scalars by value have no ctypes type; output routines: plain build
         L.orc_plot_setup.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PI, _I, _I, _PI, _PI, _PD, _PI, _PI, _PI]
         L.orc_calcjacob_8node.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
@@ -76,10 +85,11 @@ def _load(path, tangent):
     return L
 
 
-def lib(tangent: bool = False):
-    if tangent not in _libs:
-        _libs[tangent] = _load(LIB_CS if tangent else LIB, tangent)
-    return _libs[tangent]
+def lib(tangent: bool = False, count: bool = False):
+    key = "count" if count else tangent
+    if key not in _libs:
+        _libs[key] = _load(LIB_COUNT if count else (LIB_CS if tangent else LIB), tangent, count)
+    return _libs[key]
 
 
 def _p(a, t=_PD):
@@ -115,14 +125,18 @@ def metrics(N: int, ivcell: np.ndarray, xv: np.ndarray, yv: np.ndarray):
 
 class Oracle:
     """The reference's single-rank residual path on the CPU, FP64 (or its
-    complex-step tangent with ``tangent=True``)."""
+    complex-step tangent with ``tangent=True``, or the operation-count build
+    with ``count=True``)."""
 
     def __init__(self, tables, physics, skip_ideal_viscous: bool = False, ncellglob: int | None = None,
-                 tangent: bool = False):
+                 tangent: bool = False, count: bool = False):
+        if tangent and count:
+            raise ValueError("the tangent and operation-count builds are separate")
         self.N = tables.N
         self.ncell = tables.ncell
         self.tangent = tangent
-        self._L = lib(tangent)
+        self.count = count
+        self._L = lib(tangent, count)
         self.dtype = np.complex128 if tangent else np.float64
         p = Params(N=tables.N, ncell=tables.ncell, ncellglob=ncellglob or tables.ncell, vismode=physics.vismode,
                    artiv=physics.artiv, skip_ideal_viscous=int(skip_ideal_viscous), mu=physics.mu,
@@ -165,6 +179,15 @@ class Oracle:
         fs = np.ascontiguousarray(fs, dtype=self.dtype)
         assert fs.shape == (6,)
         self._L.orc_set_freestream(self._h, _p(fs))
+
+    def op_counts(self, reset: bool = True) -> dict:
+        """Operations on state-dependent quantities since the last reset
+        (operation-count build only): add (+ and -), mul, div, sqrt."""
+        if not self.count:
+            raise ValueError("op_counts needs Oracle(..., count=True)")
+        out = (ctypes.c_ulonglong * 4)()
+        self._L.orc_count_read(out, int(reset))
+        return {"add": out[0], "mul": out[1], "div": out[2], "sqrt": out[3]}
 
     def compresid(self):
         self._L.orc_compresid(self._h)
