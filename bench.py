@@ -53,6 +53,14 @@ NR, NT, NPTS = 256, 512, 5
 MS, MA = 0.5, 2.0  # Ms = 1.5 diverges within ~10 steps in the reference algorithm (AV off)
 
 
+# Operations (+, -, *, / and square roots) on state-dependent values per
+# DOF-stage of RK_S5P3 at N = 5 with mu = eta0 = 0: the reference's FP64
+# arithmetic, counted by the oracle's operation-count build on the cylinder
+# (1568.1 at 128x256, 1568.6 at 64x128; tests/test_oracle_counts.py pins the
+# count).  The FP64 side of the roofline.
+REF_OPS_PER_DOF_STAGE_N5 = 1568.0
+
+
 def bytes_per_dof_stage(N: int) -> float:
     """Algorithmic HBM bytes per DOF-stage: 3*9*8 (state in, state out, RK
     register traffic averaged over RK_S5P3) + 8 (Jac) + 32(N+1)/N (the four
@@ -306,7 +314,13 @@ def run_ours(args):
         "accuracy": acc,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "bytes_per_dof_stage": bpd, "kernel": "stage_kernel<5,8,float> (mixed)"},
+                     "bytes_per_dof_stage": bpd, "kernel": "stage_kernel<5,8,float> (mixed)",
+                     "fp64_side": {"ref_ops_per_dof_stage": REF_OPS_PER_DOF_STAGE_N5,
+                                   "ref_ops_per_byte": REF_OPS_PER_DOF_STAGE_N5 / bpd,
+                                   "fp64_form_ref_ops_per_s": val["fp64"] * REF_OPS_PER_DOF_STAGE_N5,
+                                   "fp64_exact_ref_ops_per_s": val["fp64_exact"] * REF_OPS_PER_DOF_STAGE_N5,
+                                   "note": "the reference's FP64 +,-,*,/,sqrt per DOF-stage (oracle count); "
+                                           "a division or root is one operation here, an FMA sequence on the GPU"}},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "e2e": {"value": e2e_units / (e2e_ms / 1e3), "unit": UNIT,
