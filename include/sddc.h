@@ -22,7 +22,9 @@
  *   - calls on one context are serialised on the context's CUDA stream;
  *     use one context per host thread.
  *
- * Fortran binding (ISO_C_BINDING) and ctypes stubs: INTEGRATION.md.
+ * A Fortran host binds these through an ISO_C_BINDING interface module
+ * (bind(C) interfaces with value arguments for scalars and type(c_ptr) for
+ * the context); Python binds them through ctypes (sddc_b200/solver.py).
  */
 #ifndef SDDC_H
 #define SDDC_H
@@ -197,9 +199,8 @@ int sddc_get_case_maxima(sddc_ctx *ctx, int icase, double *eigvmax, double *umax
 
 /* ---- residual evaluation without device allocation ----------------------
    No counterpart in the reference.  For callers that cannot call cudaMalloc:
-   a host that hands out all device memory from its own pool or budget, code
-   running while a stream is being captured into a CUDA graph, a plugin
-   inside a framework that owns the allocator.  The caller passes all inputs
+   a host that hands out all device memory from its own pool or budget, or a
+   plugin inside a framework that owns the allocator.  The caller passes all inputs
    and outputs as device memory it holds; the working memory (face traces,
    running-maxima slots, AV sensor, fault flags) is one fixed array of
    SDDC_NOALLOC_SCRATCH_BYTES bytes inside the library, which every GPU that

@@ -17,6 +17,7 @@
 
 #include "context_impl.h"
 #include "sd_basis.h"
+#include "tables_pack.h"
 #include "visc_kernel.cuh"
 
 using namespace sddc;
@@ -131,16 +132,7 @@ std::vector<double> sp_weights(const double *Xs, int N)
 
 }  // namespace
 
-int sddc::met_size(int N)
-{
-    switch (N) {
-    case 2: return MetLayout<2>::kSize;
-    case 3: return MetLayout<3>::kSize;
-    case 4: return MetLayout<4>::kSize;
-    case 5: return MetLayout<5>::kSize;
-    default: return MetLayout<6>::kSize;
-    }
-}
+int sddc::met_size(int N) { return met_record_doubles(N); }
 
 int sddc::set_err(sddc_ctx *c, int code, const std::string &m)
 {
@@ -297,23 +289,8 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
         }
     // packed metrics: S1(1,1:2,r,j), S2(2,1:2,i,r), Jac(i,j)
     std::vector<double> met((size_t)NC * ctx->msize, 0.0);
+    pack_metric_records(N, NC, S1, S2, Jac, met.data());
     const int kFam = 2 * N * N1, kJac = 2 * kFam;
-    for (size_t c = 0; c < (size_t)NC; c++) {
-        double *m = &met[c * ctx->msize];
-        for (int j = 0; j < N; j++)
-            for (int r = 0; r < N1; r++) {
-                const size_t b = 4 * (r + (size_t)N1 * (j + (size_t)N * c));
-                m[2 * (j * N1 + r)] = S1[b + 0];
-                m[2 * (j * N1 + r) + 1] = S1[b + 2];
-            }
-        for (int i = 0; i < N; i++)
-            for (int r = 0; r < N1; r++) {
-                const size_t b = 4 * (i + (size_t)N * (r + (size_t)N1 * c));
-                m[kFam + 2 * (i * N1 + r)] = S2[b + 1];
-                m[kFam + 2 * (i * N1 + r) + 1] = S2[b + 3];
-            }
-        for (int k = 0; k < N * N; k++) m[kJac + k] = Jac[k + (size_t)N * N * c];
-    }
     // the same, split: normals (rounded once to the form's type) and Jac
     // (its IEEE reciprocal for the forms that multiply by 1/Jac) padded to
     // an even count, so that a tile's slices are 16-byte aligned
@@ -331,52 +308,11 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
         for (int k = 0; k < N * N; k++) jac[c * NJ + k] = ctx->jac_inv ? 1.0 / m[kJac + k] : m[kJac + k];
     }
     // per-(cell, local face) records from the reference's face lists
-    std::vector<int2> fr((size_t)NC * 4, make_int2(-1, 0));
-    auto IF2 = [&](int f, int k) { return IF2C[(f - 1) + (size_t)nface * (k - 1)]; };
-    std::string msg;
-    auto claim = [&](int cell, int lf, int partner, int kind, int plf) {
-        if (cell < 1 || cell > NC || lf < 1 || lf > 4 || (partner && (partner < 1 || partner > NC)) ||
-            (partner && (plf < 1 || plf > 4))) {
-            if (msg.empty()) msg = "face list entry out of range";
-            return;
-        }
-        int2 &r = fr[(size_t)(cell - 1) * 4 + (lf - 1)];
-        if ((r.y & 0xff) != kFaceNone) {
-            if (msg.empty())
-                msg = "cell " + std::to_string(cell) + " local face " + std::to_string(lf) + " is listed twice";
-            return;
-        }
-        r = make_int2(partner ? partner - 1 : -1, kind | (plf << 8));
-    };
-    auto face_ok = [&](int f) { return f >= 1 && f <= nface; };
-    for (int k = 0; k < ninter; k++) {
-        const int f = ibfinter[k];
-        if (!face_ok(f)) { msg = "IBFINTER entry out of range"; break; }
-        claim(IF2(f, 1), IF2(f, 3), IF2(f, 2), kFaceLeft, IF2(f, 4));
-        claim(IF2(f, 2), IF2(f, 4), IF2(f, 1), kFaceRight, IF2(f, 3));
-    }
-    for (int k = 0; k < npair && msg.empty(); k++) {
-        const int f1 = cyc2fpair[k], f2 = cyc2fpair[k + npair];
-        if (!face_ok(f1) || !face_ok(f2)) { msg = "CYC2FPAIR entry out of range"; break; }
-        claim(IF2(f1, 1), IF2(f1, 3), IF2(f2, 1), kFaceLeft, IF2(f2, 3));
-        claim(IF2(f2, 1), IF2(f2, 3), IF2(f1, 1), kFaceRight, IF2(f1, 3));
-    }
-    const int *lists[5] = {ibfinl, ibfout, ibfwal, ibfsymp, ibfree};
-    const int counts[5] = {ninlet, noutlet, nwall, nsymp, nfree};
-    const int kinds[5] = {kFaceInle, kFaceOutl, kFaceWall, kFaceSymp, kFaceFree};
-    for (int t = 0; t < 5 && msg.empty(); t++)
-        for (int k = 0; k < counts[t]; k++) {
-            const int f = lists[t][k];
-            if (!face_ok(f)) { msg = "boundary list entry out of range"; break; }
-            claim(IF2(f, 1), IF2(f, 3), 0, kinds[t], 0);
-        }
-    if (msg.empty())
-        for (size_t k = 0; k < fr.size(); k++)
-            if ((fr[k].y & 0xff) == kFaceNone) {
-                msg = "cell " + std::to_string(k / 4 + 1) + " local face " + std::to_string(k % 4 + 1) +
-                      " is in no face list (processor faces do not exist on one GPU)";
-                break;
-            }
+    std::vector<int2> fr((size_t)NC * 4);
+    const FaceLists fl{IF2C, nface, ibfinter, ninter, ibfinl, ninlet, ibfout, noutlet, ibfwal, nwall,
+                       ibfsymp, nsymp, ibfree, nfree, cyc2fpair, npair};
+    static_assert(sizeof(int2) == 2 * sizeof(int), "face records are int pairs");
+    const std::string msg = build_face_records(NC, fl, reinterpret_cast<int *>(fr.data()));
     if (!msg.empty()) return set_err(ctx, SDDC_EINVAL, "sddc_set_tables: " + msg);
     std::vector<double> met2;
     if (ctx->visc) {

@@ -2,9 +2,9 @@
 //
 // For callers that cannot call cudaMalloc: a host whose device memory is all
 // handed out by its own pool or budget (a Fortran or C++ solver that
-// pre-allocates the GPU at start-up), code running while a CUDA stream is
-// being captured into a graph (cudaMalloc is not allowed there), or a
-// plugin inside another framework that owns the allocator.  The caller
+// pre-allocates the GPU at start-up), or a plugin inside another framework
+// that owns the allocator.  The call synchronises the caller's stream before
+// it returns.  The caller
 // passes every input and output as device memory it already holds; the
 // working memory the residual needs beyond those (the face traces of the
 // state, the running-maxima slots, the AV sensor and the fault flags) lives
@@ -21,6 +21,7 @@
 #include "../../include/sddc.h"
 #include "sd_basis.h"
 #include "stage_kernel.cuh"
+#include "tables_pack.h"
 
 namespace sddc {
 cudaError_t launch_stage_exact(int N, int cpb, bool diag, const StageArgs &a, const Ops &ops, cudaStream_t st);
@@ -72,7 +73,8 @@ int fail(int code, const std::string &m)
 }
 
 // device address of the scratch array on the current device, looked up once
-// per device (the first call on a device must not be inside a stream capture)
+// per device by the first call on it (that first call should come before any
+// stream capture on the device)
 int scratch_on_current_device(unsigned char **out)
 {
     int dev = 0;
@@ -100,8 +102,7 @@ extern "C" size_t sddc_noalloc_scratch_bytes(void) { return kScratchBytes; }
 extern "C" int sddc_noalloc_packed_sizes(int N, int ncell, size_t *met_doubles, size_t *face_ints)
 {
     if (N < 2 || N > kMaxN || ncell < 1) return fail(SDDC_EINVAL, "N must be in [2, 6] and ncell positive");
-    const int msize = (2 * 2 * N * (N + 1) + N * N + 1) & ~1;  // MetLayout<N>::kSize
-    if (met_doubles) *met_doubles = (size_t)ncell * msize;
+    if (met_doubles) *met_doubles = (size_t)ncell * met_record_doubles(N);
     if (face_ints) *face_ints = (size_t)ncell * 4 * 2;
     return SDDC_OK;
 }
@@ -118,64 +119,11 @@ extern "C" int sddc_noalloc_pack_tables(int N, int ncell, const double *S1, cons
     if (rc) return rc;
     if (!S1 || !S2 || !Jac || !IF2C || nface < 1 || !met_out || !faces_out)
         return fail(SDDC_EINVAL, "sddc_noalloc_pack_tables: NULL table or nface < 1");
-    const int N1 = N + 1, msize = (int)(nmet / ncell), kFam = 2 * N * N1;
-    std::memset(met_out, 0, nmet * sizeof(double));
-    for (size_t c = 0; c < (size_t)ncell; c++) {
-        double *m = met_out + c * msize;
-        for (int j = 0; j < N; j++)
-            for (int r = 0; r < N1; r++) {
-                const size_t b = 4 * (r + (size_t)N1 * (j + (size_t)N * c));
-                m[2 * (j * N1 + r)] = S1[b + 0];      // S1(1,1,r,j)
-                m[2 * (j * N1 + r) + 1] = S1[b + 2];  // S1(1,2,r,j)
-            }
-        for (int i = 0; i < N; i++)
-            for (int r = 0; r < N1; r++) {
-                const size_t b = 4 * (i + (size_t)N * (r + (size_t)N1 * c));
-                m[kFam + 2 * (i * N1 + r)] = S2[b + 1];      // S2(2,1,i,r)
-                m[kFam + 2 * (i * N1 + r) + 1] = S2[b + 3];  // S2(2,2,i,r)
-            }
-        for (int k = 0; k < N * N; k++) m[2 * kFam + k] = Jac[k + (size_t)N * N * c];
-    }
-    // per-(cell, local face) records: partner cell (0-based, -1 on a
-    // boundary) and kind | partner's local face << 8
-    for (size_t k = 0; k < (size_t)ncell * 4; k++) {
-        faces_out[2 * k] = -1;
-        faces_out[2 * k + 1] = kFaceNone;
-    }
-    auto IF2 = [&](int f, int k) { return IF2C[(f - 1) + (size_t)nface * (k - 1)]; };
-    auto claim = [&](int cell, int lf, int partner, int kind, int plf) -> bool {
-        if (cell < 1 || cell > ncell || lf < 1 || lf > 4) return false;
-        if (partner && (partner < 1 || partner > ncell || plf < 1 || plf > 4)) return false;
-        int *r = faces_out + 2 * ((size_t)(cell - 1) * 4 + (lf - 1));
-        if ((r[1] & 0xff) != kFaceNone) return false;
-        r[0] = partner ? partner - 1 : -1;
-        r[1] = kind | (plf << 8);
-        return true;
-    };
-    auto face_ok = [&](int f) { return f >= 1 && f <= nface; };
-    bool ok = true;
-    for (int k = 0; k < ninter && ok; k++) {
-        const int f = ibfinter[k];
-        ok = face_ok(f) && claim(IF2(f, 1), IF2(f, 3), IF2(f, 2), kFaceLeft, IF2(f, 4)) &&
-             claim(IF2(f, 2), IF2(f, 4), IF2(f, 1), kFaceRight, IF2(f, 3));
-    }
-    for (int k = 0; k < npair && ok; k++) {
-        const int f1 = cyc2fpair[k], f2 = cyc2fpair[k + npair];
-        ok = face_ok(f1) && face_ok(f2) && claim(IF2(f1, 1), IF2(f1, 3), IF2(f2, 1), kFaceLeft, IF2(f2, 3)) &&
-             claim(IF2(f2, 1), IF2(f2, 3), IF2(f1, 1), kFaceRight, IF2(f1, 3));
-    }
-    const int *lists[5] = {ibfinl, ibfout, ibfwal, ibfsymp, ibfree};
-    const int counts[5] = {ninlet, noutlet, nwall, nsymp, nfree};
-    const int kinds[5] = {kFaceInle, kFaceOutl, kFaceWall, kFaceSymp, kFaceFree};
-    for (int t = 0; t < 5 && ok; t++)
-        for (int k = 0; k < counts[t] && ok; k++) {
-            const int f = lists[t][k];
-            ok = face_ok(f) && claim(IF2(f, 1), IF2(f, 3), 0, kinds[t], 0);
-        }
-    if (!ok) return fail(SDDC_EINVAL, "face lists: entry out of range or a (cell, local face) listed twice");
-    for (size_t k = 0; k < (size_t)ncell * 4; k++)
-        if ((faces_out[2 * k + 1] & 0xff) == kFaceNone)
-            return fail(SDDC_EINVAL, "face lists: a (cell, local face) is in no list");
+    pack_metric_records(N, ncell, S1, S2, Jac, met_out);
+    const FaceLists fl{IF2C, nface, ibfinter, ninter, ibfinl, ninlet, ibfout, noutlet, ibfwal, nwall,
+                       ibfsymp, nsymp, ibfree, nfree, cyc2fpair, npair};
+    const std::string msg = build_face_records(ncell, fl, faces_out);
+    if (!msg.empty()) return fail(SDDC_EINVAL, "face lists: " + msg);
     return SDDC_OK;
 }
 

@@ -3,10 +3,14 @@
 ``make_cases`` draws the ensemble of the configured benchmark: cylinder
 O-grids with sizes uniform over {16x32, 32x64, 64x128, 128x256}
 (radial x circumferential), p = 3, seeded.  The configured sonic Mach range
-[0.8, 2.0] diverges within a few hundred steps in the reference algorithm
-(its artificial viscosity is computed but applied with zero coefficients),
-so the free streams are drawn with Ms in [0.2, 0.3] and the configured
-Alfven Mach range [1.5, 5.0]; each case keeps its own CFL time step.
+[0.8, 2.0] diverges in the reference algorithm (its artificial viscosity is
+computed but applied with zero coefficients, getrusanov.f90:326,328): on the
+32x64 O-grid Ms = 0.8 reaches non-positive pressure after 469 RK3 steps and
+a non-finite state after 496, Ms = 1.0 after 12 and 16, Ms = 1.5 after 4 and
+6 (tests/test_configured_mach.py on the oracle, tests/test_gpu_configured.py
+on the GPU).  The free streams are therefore drawn with Ms in [0.2, 0.3] and
+the configured Alfven Mach range [1.5, 5.0]; each case keeps its own CFL
+time step.
 
 ``merge`` concatenates the cases' set-up tables (cells, faces and face lists
 renumbered) so that one drop-in context holds the whole batch; ``Batch``

@@ -1,8 +1,8 @@
 """The allocation-free residual entry point (sddc_compresid_noalloc).
 
 Some callers cannot call cudaMalloc -- a host that hands out the GPU's memory
-from its own pool, code running during CUDA stream capture, a plugin inside a
-framework that owns the allocator.  For them the library offers one residual
+from its own pool or budget, a plugin inside a framework that owns the
+allocator.  For them the library offers one residual
 evaluation that takes every input and output as caller-held device memory
 and keeps its working memory in a fixed array inside the library.
 
@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from helpers import case_channel, case_cylinder
+from helpers import case_channel, case_cylinder, case_periodic
 from sddc_b200 import _native
 from sddc_b200.solver import Params, Solver, lib
 
@@ -71,7 +71,7 @@ def _packed(L, t):
 
 
 @pytest.mark.parametrize("precision", [0, 1, 2])
-@pytest.mark.parametrize("make", [case_cylinder, lambda: case_channel(N=5)])
+@pytest.mark.parametrize("make", [case_cylinder, lambda: case_channel(N=5), case_periodic])
 def test_noalloc_matches_regular_entry_point(make, precision):
     import torch
 
