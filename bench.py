@@ -587,15 +587,16 @@ def output_bench(torch, solver_mod, mesh, t, ph, Q0, dt, cpb, steps=200, nwrite=
     }
 
 
-def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
+def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=16, seed=0):
     """The discrete adjoint on the cylinder 128x256, p = 3 (N = 4): the
     objective is C_D averaged over the states after n1..n2 exact RK_S5P3
     steps; gradients with respect to the initial field and the inflow sonic
     and Alfven Mach numbers (through the boundary states and the initial
     field), checkpoints every 20 steps.  Cost ratio: the reverse sweep
     (recomputation and VJPs) over the plain exact forward run of the same
-    steps, both timed with CUDA events on the context's stream.  A few
-    central differences (h = 1e-6) of J check the gradient."""
+    steps, both timed with CUDA events on the context's stream.  Central
+    differences of J in 16 seeded random directions of the initial field, at
+    h = 1e-6 and at h = 1e-9, check the gradient."""
     from sddc_b200 import adjoint, cases, host, mesh
     from sddc_b200.solver import Solver
 
@@ -662,8 +663,12 @@ def adjoint_bench(torch, nsteps=1200, n1=1000, n2=1200, fd_dirs=3, seed=0):
                          if fd_dirs else None,
                          "h1e-9": {"max_rel_err": max(errs[1e-9]), "median_rel_err": float(np.median(errs[1e-9]))}
                          if fd_dirs else None,
-                         "note": "h=1e-6 crosses kinks of the running-max c_h; at h=1e-9 the rounding of J "
-                                 "over 1200 steps limits the quotient to ~1e-5"},
+                         "bar_1e-6_at_h1e-6_met": bool(fd_dirs and max(errs[1e-6]) <= 1e-6),
+                         "note": "the 1e-6 bar at h=1e-6 is not met: J is piecewise smooth (the running-max "
+                                 "c_h has thousands of kinks over 1200 steps) and a 1e-6 step moves argmaxes, so "
+                                 "the quotient averages one-sided slopes; at h=1e-9 the rounding of J over "
+                                 "1200 steps limits the quotient to ~1e-5. The adjoint equals the complex-step "
+                                 "FP64 tangent to 1e-12"},
             "tangent_check": "tests/test_gpu_adjoint.py: adjoint = complex-step FP64 CPU tangent to 1e-12 "
                              "(24x48 cells, 200 steps, 600 raised maxima)"}
 
@@ -748,7 +753,7 @@ def main():
 
         n = args.adjoint_steps
         print(json.dumps({"adjoint": adjoint_bench(torch, nsteps=n, n1=n * 5 // 6, n2=n,
-                                                   fd_dirs=3 if n >= 100 else 0)}))
+                                                   fd_dirs=16 if n >= 100 else 0)}))
         return
     if args.orszag_tang:
         import torch

@@ -128,6 +128,38 @@ int sddc_monitor(sddc_ctx *ctx, double *residsum, double *divbsum, double *mass,
 /* Running maxima after the last evaluation and the c_h used by the next. */
 int sddc_get_maxima(sddc_ctx *ctx, double *eigvmax, double *umax, double *c_h, double *ctime);
 
+/* ---- decomposed runs: one partition per rank ---------------------------
+   Replace PROCINTFLUX (procintflux_all.f90:1-155), CYCREMFLUX
+   (cycremflux_all.f90:1-155) and the MAX allreduce of compflux.f90:10-11.
+   A processor face is a face whose other cell lives on another rank
+   (IBFPROC; IF2C(K,1) and IF2C(K,3) are the own cell and its local face).
+   Each stage this rank evaluates it with its own cell as the left cell,
+   the other rank's trace as the right state, as the reference does.
+
+   sddc_set_proc_faces declares them, in exchange-slot order, before
+   sddc_set_tables (which then accepts them as covering their (cell, local
+   face)).  sddc_set_exchange gives three device buffers the host owns:
+     send_dev  [nproc][N][9]: this rank's trace of every processor face,
+               nfp ascending (the reference's SBUFC), written by the library;
+     recv_dev  [nproc][N][9]: the other ranks' traces, in their point order
+               (RBUFC), read by the library;
+     maxima_dev [2]: eigvmax, umax of this rank before, and of all ranks
+               after, the host's MAX reduction;
+   the traces in the form's arithmetic type (float in SDDC_MIXED, else
+   double).  After the traces of a new state exist (set_state, every RK
+   stage, every residual evaluation) the library fills send_dev and
+   maxima_dev on the context's stream and calls fn(user); fn enqueues the
+   exchange and the reduction on that stream (sddc_get_stream) and returns
+   0, or nonzero to fail the call.  Steps of a decomposed run are launched
+   stage by stage (no CUDA graph).  Batches, the viscous chain, the adjoint
+   and the AV sensor read back after steps (sddc_get_state muAV / sm_ind
+   after sddc_rk_step) are not available in a decomposed run;
+   sddc_compresid forms the sensor with the reduced maxima. */
+int sddc_set_proc_faces(sddc_ctx *ctx, int nproc, const int *ibfproc);
+typedef int (*sddc_exchange_fn)(void *user);
+int sddc_set_exchange(sddc_ctx *ctx, sddc_exchange_fn fn, void *user, void *send_dev, void *recv_dev,
+                      double *maxima_dev);
+
 /* Device pointer of the state (9,N,N,NCELL), valid until the next call;
    for callers that keep their data on the GPU. */
 int sddc_state_device_ptr(sddc_ctx *ctx, double **q_dev);

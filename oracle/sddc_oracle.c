@@ -74,6 +74,15 @@ struct orc_ctx {
     int *IF2C, *ibfinter, *ibfinl, *ibfout, *ibfwal, *ibfsymp, *ibfree,
         *cyc2fpair;
     int iface2fp[4 * 16], jface2fp[4 * 16]; /* (nfp,lf), N <= 16 */
+    /* processor faces of a decomposed run: IBFPROC, the own traces sent
+       (Qfl_p) and the remote traces received, in own point order (Qfr_p),
+       (9, N, NPROCINT) each (procintflux_all.f90:28-99) */
+    int nproc;
+    int *ibfproc;
+    real *Qfl_p, *Qfr_p;
+    /* the RK_S5P3 registers and stage-start time of the staged interface */
+    real *Qk0_s, *Qka_s;
+    double ctime0_s, ctime_stage_s;
     /* state and work arrays */
     real *Q, *resid, *F1, *G2, *Fv1, *Gv2, *Qvfi, *Qvfj;
     real *nablaQs, *nablaQvfi, *nablaQvfj, *dedxi, *dedeta;
@@ -363,7 +372,8 @@ void orc_destroy(orc_ctx *cx)
                     cx->cyc2fpair, cx->Q, cx->resid, cx->F1, cx->G2, cx->Fv1,
                     cx->Gv2, cx->Qvfi, cx->Qvfj, cx->nablaQs, cx->nablaQvfi,
                     cx->nablaQvfj, cx->dedxi, cx->dedeta, cx->muAV,
-                    cx->SM_IND, cx->muAVfi, cx->muAVfj};
+                    cx->SM_IND, cx->muAVfi, cx->muAVfj, cx->ibfproc,
+                    cx->Qfl_p, cx->Qfr_p, cx->Qk0_s, cx->Qka_s};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(cx);
 }
@@ -436,6 +446,14 @@ void orc_get_maxima(const orc_ctx *cx, double *eigvmax, double *umax,
     if (c_h) *c_h = RV(cx->c_h);
     if (epsilon0) *epsilon0 = cx->epsilon0;
     if (ctime) *ctime = cx->ctime;
+}
+
+/* this rank's running maxima eigvmax, umax: the operands of the MAX
+   allreduce of compflux.f90:10-11 */
+void orc_get_local_maxima(const orc_ctx *cx, double *eigvmax, double *umax)
+{
+    *eigvmax = RV(cx->eigvmax);
+    *umax = RV(cx->umax);
 }
 
 void orc_get_fluxes(const orc_ctx *cx, real *F1, real *G2, real *Fv1,
@@ -807,6 +825,83 @@ static void interface_and_cyclic_flux(orc_ctx *cx)
     }
     cx->eigvmax = em_all;
     cx->umax = um_all;
+}
+
+/* ---- processor faces of a decomposed run ------------------------------
+   PROCINTFLUX (procintflux_all.f90:1-155) and CYCREMFLUX
+   (cycremflux_all.f90:1-155) evaluate a face whose other cell lives on
+   another rank on each side, each with its own cell as the left cell: its
+   own trace and normal, sign_r = 1, the received trace as the right state
+   (point order reversed), and only Fnl scattered to its own cell. */
+int orc_set_proc_faces(orc_ctx *cx, int nproc, const int *ibfproc)
+{
+    if (nproc < 0 || (nproc > 0 && !ibfproc)) return -1;
+    for (int b = 0; b < nproc; b++)
+        if (ibfproc[b] < 1 || ibfproc[b] > cx->nface) return -1;
+    free(cx->ibfproc); free(cx->Qfl_p); free(cx->Qfr_p);
+    cx->nproc = nproc;
+    cx->ibfproc = dup_ints(ibfproc, nproc);
+    cx->Qfl_p = (real *)zalloc(sizeof(real) * NV * cx->N * (nproc > 0 ? nproc : 1));
+    cx->Qfr_p = (real *)zalloc(sizeof(real) * NV * cx->N * (nproc > 0 ? nproc : 1));
+    return 0;
+}
+
+/* the send buffers SBUFC(9*N, NPROCINT): each processor face's own trace,
+   nfp ascending, nine variables per point (procintflux_all.f90:37-76) */
+void orc_proc_pack(orc_ctx *cx, real *sbuf)
+{
+    int N = cx->N;
+    for (int b = 1; b <= cx->nproc; b++) {
+        int K = cx->ibfproc[b - 1], ic = IF2C_(K, 1), lf = IF2C_(K, 3);
+        for (int nfp = 1; nfp <= N; nfp++) {
+            int ifp, jfp;
+            real *ql = cx->Qfl_p + NV * ((nfp - 1) + N * (b - 1));
+            face_trace(cx, ic, lf, nfp, ql, &ifp, &jfp);
+            for (int k = 0; k < NV; k++) sbuf[NV * ((nfp - 1) + N * (b - 1)) + k] = ql[k];
+        }
+    }
+}
+
+/* the receive buffers RBUFC(9*N, NPROCINT), remote point nfprm going to
+   own point N+1-nfprm (procintflux_all.f90:83-99) */
+void orc_proc_unpack(orc_ctx *cx, const real *rbuf)
+{
+    int N = cx->N;
+    for (int b = 1; b <= cx->nproc; b++)
+        for (int nfprm = 1; nfprm <= N; nfprm++) {
+            int nfp = N + 1 - nfprm;
+            for (int k = 0; k < NV; k++)
+                cx->Qfr_p[NV * ((nfp - 1) + N * (b - 1)) + k] = rbuf[NV * ((nfprm - 1) + N * (b - 1)) + k];
+        }
+}
+
+/* procintflux_all.f90:104-151 */
+static void proc_flux(orc_ctx *cx)
+{
+    int N = cx->N;
+    real em = cx->eigvmax, um = cx->umax;
+    for (int b = 1; b <= cx->nproc; b++) {
+        int K = cx->ibfproc[b - 1], ic = IF2C_(K, 1), lf = IF2C_(K, 3);
+        int fam = (lf % 2) + 1;
+        for (int nfp = 1; nfp <= N; nfp++) {
+            int ifpl = IFP_(nfp, lf), jfpl = JFP_(nfp, lf);
+            int sign_l = 1;
+            real normf[2], Fnl[NV], Fnr[NV], avg[NV], eigv;
+            if (fam == 1) { if (ifpl == 1) sign_l = -1; }
+            else { if (jfpl == 1) sign_l = -1; }
+            face_normal(cx, ic, lf, ifpl, jfpl, normf);
+            const real *Qfl = cx->Qfl_p + NV * ((nfp - 1) + N * (b - 1));
+            const real *Qfr = cx->Qfr_p + NV * ((nfp - 1) + N * (b - 1));
+            rusanov(Qfl, Qfr, Fnl, Fnr, normf, sign_l, 1, cx->c_h, &eigv, &em, &um);
+            store_face(cx, cx->F1, cx->G2, ic, lf, ifpl, jfpl, Fnl);
+            if (cx->p.vismode == 1) {
+                for (int k = 0; k < NV; k++) avg[k] = 0.5 * Qfl[k] + 0.5 * Qfr[k];
+                store_face(cx, cx->Qvfi, cx->Qvfj, ic, lf, ifpl, jfpl, avg);
+            }
+        }
+    }
+    cx->eigvmax = em;
+    cx->umax = um;
 }
 
 enum { BC_INLE = 0, BC_OUTL, BC_WALL, BC_SYMP, BC_FREE };
@@ -1339,16 +1434,22 @@ static int viscous_chain_skipped(const orc_ctx *cx)
     return cx->p.skip_ideal_viscous && cx->p.mu == 0.0 && cx->p.eta0 == 0.0;
 }
 
-/* compflux, compflux.f90:1-33 */
-static void compflux(orc_ctx *cx)
+/* compflux up to its MAX allreduce, compflux.f90:6-8: c_h from the global
+   running maxima, then comp_inviscid_flux in the reference's order
+   (compflux.f90:35-51): interior flux points, interfaceflux, PROCINTFLUX
+   and CYCREMFLUX (the processor faces), CYCLOCFLUX, BCFLUX */
+static void compflux_local(orc_ctx *cx)
 {
     cx->c_h = r_sqrt(cx->eigvmax_g * (cx->eigvmax_g - cx->umax_g));
     inviscid_flux_interior(cx);
     interface_and_cyclic_flux(cx);
+    proc_flux(cx);
     bcflux(cx);
-    /* single rank: MPI_ALLREDUCE(MAX) is the identity (compflux.f90:10-11) */
-    cx->eigvmax_g = cx->eigvmax;
-    cx->umax_g = cx->umax;
+}
+
+/* compflux after the allreduce (compflux.f90:13-31) */
+static void compflux_finish(orc_ctx *cx)
+{
     if (cx->p.vismode == 1) {
         nablaQsp(cx);
         int skip = viscous_chain_skipped(cx);
@@ -1373,10 +1474,45 @@ static void compflux(orc_ctx *cx)
     }
 }
 
+/* compflux, compflux.f90:1-33 */
+static void compflux(orc_ctx *cx)
+{
+    compflux_local(cx);
+    /* single rank: MPI_ALLREDUCE(MAX) is the identity (compflux.f90:10-11) */
+    cx->eigvmax_g = cx->eigvmax;
+    cx->umax_g = cx->umax;
+    compflux_finish(cx);
+}
+
+static void compresid_divergence(orc_ctx *cx);
+
 /* compresid, compresid.f90:1-80 */
 void orc_compresid(orc_ctx *cx)
 {
     compflux(cx);
+    compresid_divergence(cx);
+}
+
+/* A residual of a decomposed run in the two halves around the MAX
+   allreduce of compflux.f90:10-11, which the caller performs over the ranks
+   between them (orc_get_maxima, then orc_set_global_maxima). */
+void orc_compresid_local(orc_ctx *cx) { compflux_local(cx); }
+
+void orc_set_global_maxima(orc_ctx *cx, double eigvmax_g, double umax_g)
+{
+    cx->eigvmax_g = eigvmax_g;
+    cx->umax_g = umax_g;
+}
+
+void orc_compresid_finish(orc_ctx *cx)
+{
+    compflux_finish(cx);
+    compresid_divergence(cx);
+}
+
+/* compresid.f90:12-78: the flux divergence over Jac and the sources */
+static void compresid_divergence(orc_ctx *cx)
+{
     int N = cx->N, N1 = cx->N1, NC = cx->NC;
     int vis = cx->p.vismode == 1, skip = viscous_chain_skipped(cx);
     real alpha = cx->alpha;
@@ -1505,6 +1641,41 @@ void orc_rk_s5p3(orc_ctx *cx, double dt, int nsteps)
     }
     free(Qk0);
     free(Qka);
+}
+
+/* RK_S5P3 one stage at a time, for a decomposed run whose ranks exchange
+   traces and maxima between the stages: orc_rk_s5p3_begin_stage, the
+   residual (orc_compresid, or its two halves around the allreduce), then
+   orc_rk_s5p3_end_stage.  The same registers and time bookkeeping as
+   orc_rk_s5p3 (iterations.f90:175-212). */
+void orc_rk_s5p3_begin_stage(orc_ctx *cx, int stage)
+{
+    long n = (long)NV * cx->N * cx->N * cx->NC;
+    if (!cx->Qk0_s) {
+        cx->Qk0_s = (real *)zalloc(sizeof(real) * n);
+        cx->Qka_s = (real *)zalloc(sizeof(real) * n);
+    }
+    if (stage == 1) {
+        memcpy(cx->Qk0_s, cx->Q, sizeof(real) * n);
+        cx->ctime0_s = cx->ctime;
+    }
+}
+
+void orc_rk_s5p3_end_stage(orc_ctx *cx, int stage, double dt)
+{
+    long n = (long)NV * cx->N * cx->N * cx->NC;
+    orc_rk_s5p3_combine(stage, n, dt, cx->Q, cx->Qk0_s, cx->Qka_s, cx->resid);
+    double d;
+    switch (stage) {
+    case 1: d = B10 * dt; break;
+    case 2: d = cx->ctime_stage_s + B21 * dt; break;
+    case 3: d = A32 * cx->ctime_stage_s + B32 * dt; break;
+    case 4: d = A43 * cx->ctime_stage_s + B43 * dt; break;
+    default: d = dt; break;
+    }
+    cx->ctime_stage_s = d;
+    cx->ctime = cx->ctime0_s + d;
+    if (stage == 2) memcpy(cx->Qka_s, cx->Q, sizeof(real) * n);
 }
 
 /* FiveStageRk, iterations.f90:88-156 */

@@ -103,6 +103,22 @@ void orc_five_stage_rk(orc_ctx *c, double dt, int nsteps); /* :88-156 */
 /* monitor sums of iterations.f90:34-46 (local, before the gather) */
 void orc_monitor(const orc_ctx *c, double *residsum, double *divbsum);
 
+/* --- decomposed runs (the reference's MPI partitions) ------------------
+   Processor faces (IBFPROC; IF2C(K,1) and IF2C(K,3) name the own cell and
+   its local face) take the remote trace from the receive buffer; a stage
+   is pack -> exchange -> unpack -> orc_compresid_local -> MAX allreduce of
+   orc_get_maxima's eigvmax, umax -> orc_set_global_maxima ->
+   orc_compresid_finish. */
+int orc_set_proc_faces(orc_ctx *c, int nproc, const int *ibfproc);
+void orc_proc_pack(orc_ctx *c, orc_real *sbuf);           /* (9, N, nproc) */
+void orc_proc_unpack(orc_ctx *c, const orc_real *rbuf);   /* (9, N, nproc) */
+void orc_compresid_local(orc_ctx *c);
+void orc_get_local_maxima(const orc_ctx *c, double *eigvmax, double *umax);
+void orc_set_global_maxima(orc_ctx *c, double eigvmax_g, double umax_g);
+void orc_compresid_finish(orc_ctx *c);
+void orc_rk_s5p3_begin_stage(orc_ctx *c, int stage);
+void orc_rk_s5p3_end_stage(orc_ctx *c, int stage, double dt);
+
 /* --- point kernels, exposed for consistency tests --------------------- */
 void orc_point_iflux(const orc_real *Qi, orc_real c_h, orc_real *umax,
                      orc_real *F, orc_real *G);

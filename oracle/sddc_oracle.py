@@ -72,6 +72,15 @@ def _load(path, tangent, count=False):
     L.orc_setsandpoints.argtypes = [_I, _PD, _PD]
     L.orc_compute_LM.argtypes = [_I, _PD, _PD, _PD, _PD]
     L.orc_calcjacob_bilinear.argtypes = [_I, _I, _PI, _PD, _PD, _PD, _PD, _PD]
+    L.orc_set_proc_faces.argtypes = [ctypes.c_void_p, _I, _PI]
+    L.orc_proc_pack.argtypes = [ctypes.c_void_p, _PD]
+    L.orc_proc_unpack.argtypes = [ctypes.c_void_p, _PD]
+    L.orc_compresid_local.argtypes = [ctypes.c_void_p]
+    L.orc_get_local_maxima.argtypes = [ctypes.c_void_p, _PD, _PD]
+    L.orc_set_global_maxima.argtypes = [ctypes.c_void_p, _D, _D]
+    L.orc_compresid_finish.argtypes = [ctypes.c_void_p]
+    L.orc_rk_s5p3_begin_stage.argtypes = [ctypes.c_void_p, _I]
+    L.orc_rk_s5p3_end_stage.argtypes = [ctypes.c_void_p, _I, _D]
     if count:  # the operation-count build: the residual path only
         L.orc_count_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), _I]
         return L
@@ -225,6 +234,45 @@ class Oracle:
         a, b = _D(), _D()
         self._L.orc_monitor(self._h, ctypes.byref(a), ctypes.byref(b))
         return a.value, b.value
+
+    # -- decomposed runs: one rank of a partitioned case ---------------------
+    def set_proc_faces(self, ibfproc):
+        """The processor faces (local face ids, 1-based, in slot order)."""
+        self._ibfproc = np.ascontiguousarray(ibfproc, dtype=np.int32)
+        rc = self._L.orc_set_proc_faces(self._h, len(self._ibfproc), _p(self._ibfproc, _PI))
+        if rc:
+            raise ValueError("orc_set_proc_faces rejected the list")
+
+    def proc_pack(self):
+        """The send buffer (nproc, N, 9): own traces, nfp ascending."""
+        buf = np.zeros((len(self._ibfproc), self.N, 9), dtype=self.dtype)
+        self._L.orc_proc_pack(self._h, _p(buf))
+        return buf
+
+    def proc_unpack(self, rbuf):
+        rbuf = np.ascontiguousarray(rbuf, dtype=self.dtype)
+        assert rbuf.shape == (len(self._ibfproc), self.N, 9)
+        self._L.orc_proc_unpack(self._h, _p(rbuf))
+
+    def compresid_local(self):
+        self._L.orc_compresid_local(self._h)
+
+    def local_maxima(self):
+        e, u = _D(), _D()
+        self._L.orc_get_local_maxima(self._h, ctypes.byref(e), ctypes.byref(u))
+        return e.value, u.value
+
+    def set_global_maxima(self, eigvmax, umax):
+        self._L.orc_set_global_maxima(self._h, float(eigvmax), float(umax))
+
+    def compresid_finish(self):
+        self._L.orc_compresid_finish(self._h)
+
+    def rk_begin_stage(self, stage):
+        self._L.orc_rk_s5p3_begin_stage(self._h, int(stage))
+
+    def rk_end_stage(self, stage, dt):
+        self._L.orc_rk_s5p3_end_stage(self._h, int(stage), float(dt))
 
     def wall_force(self, w):
         """(Fx, Fy) on the wall faces at the current state; w = quadrature

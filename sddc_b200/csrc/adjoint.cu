@@ -196,6 +196,8 @@ int check_adjoint_ctx(sddc_ctx *ctx)
     if (ctx->ncase) return set_err(ctx, SDDC_ESTATE, "the adjoint runs one case (no batch)");
     if (ctx->p.k_stage != 3) return set_err(ctx, SDDC_EINVAL, "the adjoint differentiates RK_S5P3 (k_stage = 3)");
     if (ctx->visc) return set_err(ctx, SDDC_EINVAL, "the adjoint differentiates the ideal chain (mu = eta0 = 0)");
+    if (!ctx->ibfproc.empty() || ctx->exch)
+        return set_err(ctx, SDDC_ESTATE, "the adjoint runs a whole case on one GPU (no processor faces)");
     return ensure_ws(ctx);
 }
 

@@ -160,7 +160,7 @@ static void free_all(sddc_ctx *ctx)
     void *bufs[] = {ctx->met, ctx->nrm, ctx->jac, ctx->faces, ctx->maxima, ctx->sm_ind, ctx->muav, ctx->resid, ctx->grad,
                     ctx->mon_part, ctx->mon_out, ctx->int_part, ctx->wq, ctx->err_flags,
                     ctx->case_dev, ctx->tiles_rk, ctx->tiles_diag, ctx->visc_grad, ctx->visc_gt,
-                    ctx->visc_rv, ctx->met2, ctx->max_scratch};
+                    ctx->visc_rv, ctx->met2, ctx->max_scratch, ctx->proc_cells};
     for (void *b : bufs) cudaFree(b);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     adjoint_free(ctx);
@@ -309,11 +309,27 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
     }
     // per-(cell, local face) records from the reference's face lists
     std::vector<int2> fr((size_t)NC * 4);
-    const FaceLists fl{IF2C, nface, ibfinter, ninter, ibfinl, ninlet, ibfout, noutlet, ibfwal, nwall,
-                       ibfsymp, nsymp, ibfree, nfree, cyc2fpair, npair};
+    FaceLists fl{IF2C, nface, ibfinter, ninter, ibfinl, ninlet, ibfout, noutlet, ibfwal, nwall,
+                 ibfsymp, nsymp, ibfree, nfree, cyc2fpair, npair};
+    fl.ibfproc = ctx->ibfproc.data();
+    fl.nproc = (int)ctx->ibfproc.size();
     static_assert(sizeof(int2) == 2 * sizeof(int), "face records are int pairs");
     const std::string msg = build_face_records(NC, fl, reinterpret_cast<int *>(fr.data()));
     if (!msg.empty()) return set_err(ctx, SDDC_EINVAL, "sddc_set_tables: " + msg);
+    if (!ctx->ibfproc.empty()) {
+        // each exchange slot's own (cell, local face), IF2C(K,1) and IF2C(K,3)
+        std::vector<int2> pc(ctx->ibfproc.size());
+        for (size_t b = 0; b < pc.size(); b++) {
+            const int K = ctx->ibfproc[b];
+            pc[b] = make_int2(IF2C[K - 1] - 1, IF2C[(K - 1) + (size_t)nface * 2]);
+        }
+        cudaFree(ctx->proc_cells);
+        ctx->proc_cells = nullptr;
+        int rc = alloc(ctx, (void **)&ctx->proc_cells, pc.size() * sizeof(int2), "processor faces");
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->proc_cells, pc.data(), pc.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    }
     std::vector<double> met2;
     if (ctx->visc) {
         // the normal row the adiabatic-wall gradient state reads
@@ -356,6 +372,82 @@ extern "C" int sddc_set_tables(sddc_ctx *ctx, const double *Lmat, const double *
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->tables = true;
     ctx->traces_stale = true;
+    ctx->proc_stale = true;
+    return SDDC_OK;
+}
+
+// ---------------------------------------------------------- decomposed runs
+
+extern "C" int sddc_set_proc_faces(sddc_ctx *ctx, int nproc, const int *ibfproc)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (ctx->tables) return set_err(ctx, SDDC_ESTATE, "sddc_set_proc_faces comes before sddc_set_tables");
+    if (nproc < 0 || (nproc > 0 && !ibfproc)) return set_err(ctx, SDDC_EINVAL, "sddc_set_proc_faces: bad list");
+    if (ctx->visc) return set_err(ctx, SDDC_EINVAL, "decomposed runs need the ideal chain (mu = eta0 = 0)");
+    ctx->ibfproc.assign(ibfproc, ibfproc + nproc);
+    return SDDC_OK;
+}
+
+extern "C" int sddc_set_exchange(sddc_ctx *ctx, sddc_exchange_fn fn, void *user, void *send_dev, void *recv_dev,
+                                 double *maxima_dev)
+{
+    if (!ctx) return SDDC_EINVAL;
+    if (!ctx->tables) return set_err(ctx, SDDC_ESTATE, "sddc_set_exchange comes after sddc_set_tables");
+    if (ctx->ncase) return set_err(ctx, SDDC_ESTATE, "a batch is not decomposed");
+    if (!fn || !maxima_dev || (!ctx->ibfproc.empty() && (!send_dev || !recv_dev)))
+        return set_err(ctx, SDDC_EINVAL, "sddc_set_exchange: NULL function or buffer");
+    ctx->exch = fn;
+    ctx->exch_user = user;
+    ctx->proc_send = send_dev;
+    ctx->proc_recv = recv_dev;
+    ctx->proc_max = maxima_dev;
+    ctx->proc_stale = true;
+    return SDDC_OK;
+}
+
+namespace {
+// send[slot][nfp][k] = trace of the slot's own (cell, local face), the
+// reference's SBUFC order (procintflux_all.f90:49-70)
+template <typename T>
+__global__ void proc_pack_kernel(int nproc, int N, const int2 *__restrict__ pc, const T *__restrict__ tr,
+                                 T *__restrict__ send)
+{
+    const int n = nproc * N * 9;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int k = e % 9, nfp0 = (e / 9) % N, b = e / (9 * N);
+        const int2 c = pc[b];
+        send[e] = tr[((size_t)c.x * 4 + (c.y - 1)) * 9 * N + (size_t)k * N + nfp0];  // trace_at
+    }
+}
+}  // namespace
+
+// The exchange of a decomposed run after the traces of register `reg`
+// exist and the running maxima of `slot` are this rank's: pack, hand the
+// maxima to the host buffer, call the host, take the reduced maxima back.
+static int exchange(sddc_ctx *ctx, int reg, int slot)
+{
+    const int nproc = (int)ctx->ibfproc.size();
+    if (!ctx->exch) {
+        if (nproc) return set_err(ctx, SDDC_ESTATE, "processor faces need sddc_set_exchange");
+        return SDDC_OK;
+    }
+    if (nproc) {
+        const int n = nproc * ctx->N * 9, nb = std::min((n + 255) / 256, 4096);
+        if (ctx->p.precision == SDDC_MIXED)
+            proc_pack_kernel<float><<<nb, 256, 0, ctx->stream>>>(
+                nproc, ctx->N, ctx->proc_cells, reinterpret_cast<const float *>(ctx->trace[reg]),
+                reinterpret_cast<float *>(ctx->proc_send));
+        else
+            proc_pack_kernel<double><<<nb, 256, 0, ctx->stream>>>(
+                nproc, ctx->N, ctx->proc_cells, reinterpret_cast<const double *>(ctx->trace[reg]),
+                reinterpret_cast<double *>(ctx->proc_send));
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(ctx->proc_max, ctx->maxima + 2 * slot, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    if (ctx->exch(ctx->exch_user) != 0) return set_err(ctx, SDDC_ECUDA, "the host's exchange failed");
+    CK(cudaMemcpyAsync(ctx->maxima + 2 * slot, ctx->proc_max, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
     return SDDC_OK;
 }
 
@@ -395,6 +487,7 @@ extern "C" int sddc_set_state(sddc_ctx *ctx, const double *Q, double ctime, doub
     ctx->ctime = ctime;
     ctx->slot = 0;
     ctx->state = true;
+    ctx->proc_stale = true;
     return SDDC_OK;
 }
 
@@ -411,6 +504,7 @@ StageArgs sddc::base_args(sddc_ctx *ctx)
     a.jac = ctx->jac;
     a.jac_inv = ctx->jac_inv ? 1 : 0;
     a.faces = ctx->faces;
+    a.proc_recv = ctx->proc_recv;
     a.maxima = ctx->maxima;
     a.sm_ind = ctx->sm_ind;
     a.err_flags = ctx->err_flags;
@@ -471,6 +565,17 @@ int sddc::ready(sddc_ctx *ctx)
     return SDDC_OK;
 }
 
+// before a residual evaluation of a decomposed run: the exchange of the
+// current state's traces, once after set_state or set_tables
+static int proc_ready(sddc_ctx *ctx)
+{
+    if (!ctx->proc_stale) return SDDC_OK;
+    int rc = exchange(ctx, 0, ctx->slot);
+    if (rc) return rc;
+    ctx->proc_stale = false;
+    return SDDC_OK;
+}
+
 int sddc::check_flags(sddc_ctx *ctx)
 {
     CK(cudaMemcpyAsync(ctx->host_small, ctx->err_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
@@ -492,6 +597,7 @@ int sddc::check_flags(sddc_ctx *ctx)
 extern "C" int sddc_compresid(sddc_ctx *ctx)
 {
     int rc = ready(ctx);
+    if (!rc) rc = proc_ready(ctx);
     if (rc) return rc;
     const size_t nc = ctx->ncell;
     if (!ctx->resid) {
@@ -510,6 +616,8 @@ extern "C" int sddc_compresid(sddc_ctx *ctx)
     a.grad_out = ctx->grad;
     a.mon_part = ctx->mon_part;
     CK(launch(ctx, true, a));
+    // a decomposed run reduces the maxima over the ranks (compflux.f90:10-11)
+    if ((rc = exchange(ctx, 0, a.slot_w))) return rc;
     ctx->slot = a.slot_w;
     ctx->sensor_stale = false;
     ctx->mon_nblk = ctx->ncase ? ctx->ntiles_diag : (ctx->ncell + 7) / 8;
@@ -517,8 +625,10 @@ extern "C" int sddc_compresid(sddc_ctx *ctx)
     return check_flags(ctx);
 }
 
-// the launches of one time step, starting from running-max slot s0
-static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
+// the launches of one time step, starting from running-max slot s0; in a
+// decomposed run (xrc not null) each stage is followed by the exchange of its
+// output's traces and maxima, whose status goes to *xrc
+static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0, int *xrc = nullptr)
 {
     double **P = ctx->reg;
     StageArgs a = base_args(ctx);
@@ -565,6 +675,7 @@ static cudaError_t enqueue_step(sddc_ctx *ctx, double dt, int s0)
         a.mon_part = k == 4 ? ctx->mon_part : nullptr;
         cudaError_t e = launch(ctx, false, a);
         if (e != cudaSuccess) return e;
+        if (xrc && (*xrc = exchange(ctx, st[k].out, a.slot_w))) return cudaSuccess;
     }
     return cudaSuccess;
 }
@@ -592,6 +703,22 @@ extern "C" int sddc_rk_step_cases(sddc_ctx *ctx, int nsteps)
 
 static int run_steps(sddc_ctx *ctx, double dt, int nsteps)
 {
+    if (ctx->exch || !ctx->ibfproc.empty()) {
+        // a decomposed run: stage by stage, the host's exchange between them
+        int rc = proc_ready(ctx);
+        if (rc) return rc;
+        for (int s = 0; s < nsteps; s++) {
+            int xrc = 0;
+            cudaError_t e = enqueue_step(ctx, dt, ctx->slot, &xrc);
+            if (e != cudaSuccess) return cuda_err(ctx, e, "stage launch");
+            if (xrc) return xrc;
+            ctx->ctime += dt;
+            ctx->sensor_stale = true;
+            ctx->mon_nblk = ctx->grid;
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+        return check_flags(ctx);
+    }
     for (int s = 0; s < nsteps; s++) {
         const int s0 = ctx->slot;
         cudaGraphExec_t &g = ctx->graph[s0];
@@ -651,6 +778,9 @@ static int refresh_sensor(sddc_ctx *ctx)
 // muAV (2,NCELL) of the current state into ctx->muav, on the stream
 int sddc::device_muav(sddc_ctx *ctx)
 {
+    if (ctx->sensor_stale && ctx->exch && ctx->p.artiv == 1 && ctx->p.vismode == 1)
+        return set_err(ctx, SDDC_ESTATE,
+                       "the AV sensor after steps of a decomposed run is not formed; call sddc_compresid first");
     if (ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
         int rc = refresh_sensor(ctx);
         if (rc) return rc;
@@ -666,6 +796,9 @@ extern "C" int sddc_get_state(sddc_ctx *ctx, double *Q, double *resid, double *n
                               double *sm_ind)
 {
     if (!ctx) return SDDC_EINVAL;
+    if ((sm_ind || muAV) && ctx->sensor_stale && ctx->exch && ctx->p.artiv == 1 && ctx->p.vismode == 1)
+        return set_err(ctx, SDDC_ESTATE,
+                       "the AV sensor after steps of a decomposed run is not formed; call sddc_compresid first");
     if (sm_ind && ctx->sensor_stale && ctx->p.artiv == 1 && ctx->p.vismode == 1) {
         int rc = refresh_sensor(ctx);
         if (rc) return rc;
@@ -761,6 +894,7 @@ static int build_tiles(sddc_ctx *ctx, int cpb, int4 **dev, int *count)
 extern "C" int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases)
 {
     if (ctx && ctx->visc) return set_err(ctx, SDDC_EINVAL, "batches run the ideal chain only (mu = eta0 = 0)");
+    if (ctx && (ctx->exch || !ctx->ibfproc.empty())) return set_err(ctx, SDDC_ESTATE, "a batch is not decomposed");
     if (!ctx || ncase < 1 || !cases) return set_err(ctx, SDDC_EINVAL, "sddc_set_cases: bad arguments");
     // the cases must tile the cell range in order
     int next = 0;

@@ -106,6 +106,14 @@ struct sddc_ctx {
     double *met2 = nullptr;       // [cell][lf][nfp][2]: the other normal row at each face point
     // restart / Tecplot output (output.cu), created on first use
     sddc::Output *out = nullptr;
+    // decomposed run: processor faces (slot order) and the host's exchange
+    std::vector<int> ibfproc;
+    int2 *proc_cells = nullptr;  // [slot]: own cell (0-based), own local face
+    sddc_exchange_fn exch = nullptr;
+    void *exch_user = nullptr;
+    void *proc_send = nullptr, *proc_recv = nullptr;
+    double *proc_max = nullptr;
+    bool proc_stale = false;  // the exchange of the current state's traces is due
 };
 
 

@@ -219,7 +219,11 @@ enum FaceKind : int {
     kFaceOutl = 4,
     kFaceWall = 5,
     kFaceSymp = 6,
-    kFaceFree = 7
+    kFaceFree = 7,
+    // processor face of a decomposed run (PROCINTFLUX / CYCREMFLUX): the
+    // other cell is on another rank; the record's partner field is the
+    // face's slot in the exchange buffers
+    kFaceProc = 8
 };
 
 // Boundary ghost states of BCFLUX (bcflux.f90:17-375).

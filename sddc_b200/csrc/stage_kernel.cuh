@@ -105,6 +105,9 @@ struct StageArgs {
     const double *__restrict__ jac;
     int jac_inv;                       // jac holds 1/Jac (the forms other than the exact one)
     const int2 *__restrict__ faces;    // (cell, local face) records
+    // remote traces of the processor faces of a decomposed run, [slot][nfp][9]
+    // in the sending rank's point order (procintflux_all.f90:83-99)
+    const void *__restrict__ proc_recv;
     double *maxima;                    // [5][2]: running max of eigv, umax
     double *__restrict__ sm_ind;       // (2,NCELL) AV sensor
     double *__restrict__ resid_out;    // (9,N,N,NCELL), residual evaluation only (null: not kept)
@@ -245,9 +248,10 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    // sQ, sA, sJac; the sensor's sJz and sLow in residual evaluations only
-    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) + 4 * 32 +
-               2 * (N - 1) * N;
+    // sQ and sJac; the residual staging sA and the sensor's sJz and sLow in
+    // residual evaluations only (a time step forms its output over sQ)
+    size_t d = (size_t)CPB * ((DIAG ? 2 : 1) * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) +
+               4 * 32 + 2 * (N - 1) * N;
     size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam) + 2 * (N + 1) * N;
     return d * sizeof(double) + r * sizeof(R);
 }
@@ -290,9 +294,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *sJz = sJac + CPB * NJ;                               // [CPB][NN]  Jz^2 for the sensor (DIAG)
     double *sLow = sJz + (DIAG ? CPB * NN : 0);                  // [CPB][kLow] (DIAG)
     double *sRed = sLow + (DIAG ? CPB * S::kLow : 0);            // [4][32] block reductions
-    // residual (DIAG); in a time step the RK register, then the output
-    double *sA = sRed + 4 * 32;                                  // [CPB][NQ]
-    double *sOpH = sA + CPB * NQ;                                // [N-1][N]  AV projection
+    double *sA = sRed + 4 * 32;                                  // [CPB][NQ] residual (DIAG only)
+    double *sOpH = sA + (DIAG ? CPB * NQ : 0);                   // [N-1][N]  AV projection
     double *sOpHL = sOpH + (N - 1) * N;                          // [N][N-1]  AV prolongation
     R *sNrm = reinterpret_cast<R *>(sOpHL + N * (N - 1));        // [CPB][NM] flux-point normals
     R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
@@ -323,10 +326,10 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     // ---- stage the state, the metrics and the operators ------------------------
     // The tile's state slice goes to sQ, its normals to sNrm and Jac to sJac
     // (or, without the split metric arrays, its packed metric records to the
-    // flux buffer, free until phase A, for conversion) and, in a stage that
-    // reads one RK register, that register's slice to sA, by TMA bulk copies
-    // that one thread issues when every slice is 16-byte aligned; otherwise
-    // by batches of loads.
+    // flux buffer, free until phase A, for conversion) by TMA bulk copies that
+    // one thread issues when every slice is 16-byte aligned; otherwise by
+    // batches of loads.  In a stage that reads one RK register, that
+    // register's slice is brought into L2 now and read by phase C's threads.
     __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sAbort;
     double *sMetRaw = reinterpret_cast<double *>(sF);
@@ -343,13 +346,12 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     const double *rsrc = want_ra ? a.reg_a + (size_t)c0 * NQ : nullptr;
     const bool bulk = ((uintptr_t)qsrc & 15) == 0 && (qbytes & 15) == 0 &&
                       (split ? (((uintptr_t)nsrc | (uintptr_t)jsrc | nbytes | jbytes) & 15) == 0
-                             : (((uintptr_t)msrc0 | mbytes) & 15) == 0) &&
-                      (!want_ra || ((uintptr_t)rsrc & 15) == 0);  // uniform in the CTA
+                             : (((uintptr_t)msrc0 | mbytes) & 15) == 0);  // uniform in the CTA
     if (tid == 0) {
         sAbort = 0;
         if (bulk) {
             mbar_init(&sBar, 1);
-            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes + (want_ra ? qbytes : 0)));
+            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes));
             bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
             if (split) {
                 bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
@@ -357,8 +359,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             } else {
                 bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
             }
-            if (want_ra) bulk_g2s(sA, rsrc, (unsigned)qbytes, &sBar);
         }
+        if (want_ra && ((uintptr_t)rsrc & 15) == 0 && (qbytes & 15) == 0) bulk_prefetch_l2(rsrc, (unsigned)qbytes);
     }
     for (int k = tid; k < NP * N; k += NT) {
         sOpL[k] = opL<R>(ops, k);
@@ -389,7 +391,6 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         } else {
             stage_copy(sMetRaw, msrc0, ncl * ML::kSize);
         }
-        if (want_ra) stage_copy(sA, rsrc, ncl * NQ);
     }
     const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
@@ -479,7 +480,17 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         int sign_l, sign_r;
         const bool pair = kind == kFaceLeft || kind == kFaceRight;
         const bool own_right = kind == kFaceRight;
-        if (pair) {
+        if (kind == kFaceProc) {
+            // PROCINTFLUX / CYCREMFLUX (procintflux_all.f90:104-151): this
+            // cell is the left cell, with its own normal and sign_r = 1; the
+            // right state is the received trace, remote point N+1-nfp
+            const R *rv = reinterpret_cast<const R *>(a.proc_recv) + ((size_t)rec.x * N + (N - nfp)) * 9;
+#pragma unroll
+            for (int k = 0; k < 9; k++) other[k] = rv[k];
+            n0 = onrm[0]; n1 = onrm[1];
+            sign_l = r == 0 ? -1 : 1;
+            sign_r = 1;
+        } else if (pair) {
             // partner point N-nfp+1 on the partner's local face; its trace was
             // published by the stage that produced q_in
             const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
@@ -699,43 +710,53 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             for (int k = 0; k < 9; k++) part_r += res[k] * res[k];
             part_d += divB * divB;
         }
-        double *ap = sA + c * NQ + 9 * (i + N * j);
         if constexpr (DIAG) {
             // stage the residual for phase E's copy-out
+            double *ap = sA + c * NQ + 9 * (i + N * j);
 #pragma unroll
             for (int k = 0; k < 9; k++) ap[k] = res[k];
         } else {
-            // ---- E: the RK stage update of this point (iterations.f90:88-213);
-            // the point's state and RK register slot are read by this thread
-            // only, so the output goes to the register slot in place, and in
-            // the float form a float copy over the state slot for phase F
-            // element by element in order: float copy k overwrites bytes of
-            // state element k/2 <= k, already read
-            const size_t g = (size_t)cell * NQ + 9 * (i + N * j);
-            const int kind = a.rk_kind;
-            R *qf = reinterpret_cast<R *>(sQ + c * NQ + 9 * (i + N * j));
+            // in a time step the residual goes, in the arithmetic type, over
+            // this point's xi-derivative slot (slot i of xi-line j), which no
+            // other thread reads; phase E takes it from there
+            R *rp = sF + c * S::kF + (0 * N + j) * NP * 9 + i * 9;
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
-                const double qk = q[k], r = res[k];
-                double o;
-                switch (kind) {
-                case kRkAxpy: o = qk + cf[0] * r; break;
-                case kRkTwoReg: o = (cf[1] * ap[k] + cf[2] * qk) + cf[0] * r; break;
-                case kRkTwoRegT: o = (cf[1] * ap[k] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
-                default:
-                    o = ((((cf[1] * a.reg_a[g + k] + cf[2] * a.reg_b[g + k]) + cf[3] * a.reg_c[g + k]) + cf[4] * qk) +
-                         cf[5] * a.reg_d[g + k]) +
-                        cf[0] * r;
-                    break;
-                }
-                ap[k] = o;
-                if (a.resid_w) a.resid_w[g + k] = r;
-                if constexpr (sizeof(R) != sizeof(double)) qf[k] = (R)o;
-            }
-            fence_proxy_async();  // sA is the source of the bulk store below
+            for (int k = 0; k < 9; k++) rp[k] = (R)res[k];
         }
     }
     __syncthreads();
+
+    // ---- E: the RK stage update (iterations.f90:88-213), element by element -----
+    // over the tile's slice: the state element (sQ), the residual (its point's
+    // xi-derivative slot) and the RK registers the stage reads (consecutive
+    // threads read consecutive register elements); the output goes over the
+    // state element in sQ, the source of the bulk store and of phase F
+    if constexpr (!DIAG) {
+        const size_t g0 = (size_t)c0 * NQ;
+        const int kind = a.rk_kind;
+        for (int e = tid; e < ncl * NQ; e += NT) {
+            const int k = e % 9, pt = e / 9;  // pt = c * NN + i + N * j
+            const int c = pt / NN, ij = pt - c * NN, i = ij % N, j = ij / N;
+            const double qk = sQ[e];
+            const double r = (double)sF[c * S::kF + (0 * N + j) * NP * 9 + i * 9 + k];
+            const size_t g = g0 + e;
+            double o;
+            switch (kind) {
+            case kRkAxpy: o = qk + cf[0] * r; break;
+            case kRkTwoReg: o = (cf[1] * a.reg_a[g] + cf[2] * qk) + cf[0] * r; break;
+            case kRkTwoRegT: o = (cf[1] * a.reg_a[g] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
+            default:
+                o = ((((cf[1] * a.reg_a[g] + cf[2] * a.reg_b[g]) + cf[3] * a.reg_c[g]) + cf[4] * qk) +
+                     cf[5] * a.reg_d[g]) +
+                    cf[0] * r;
+                break;
+            }
+            sQ[e] = o;
+            if (a.resid_w) a.resid_w[g] = r;
+        }
+        fence_proxy_async();  // sQ is the source of the bulk store below
+        __syncthreads();
+    }
 
     // ---- D: AV smoothness sensor (comp_artificial_viscosity, AV.f90:14-83) ------
     const bool av = DIAG && a.artiv == 1 && a.vismode == 1;
@@ -821,7 +842,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         }
     }
 
-    // ---- E: residual copy-out (residual evaluation) or the output store ---------
+    // ---- residual copy-out (residual evaluation) or the output store ----------
     const double *qout_src = nullptr;
     bool out_bulk = false;
     {
@@ -831,17 +852,17 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             if (a.resid_out)
                 for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sA[e];
         } else {
-            // the output slice (formed in sA by phase C) to q_out: one bulk
+            // the output slice (formed over sQ by phase E) to q_out: one bulk
             // store issued by one thread, read from shared memory while phase
             // F runs, or coalesced stores when the slice is not 16-byte aligned
             double *dst = a.q_out + g0;
             out_bulk = (((uintptr_t)dst | (size_t)n * sizeof(double)) & 15) == 0;
             if (out_bulk) {
-                if (tid == 0) bulk_s2g(dst, sA, (unsigned)(n * sizeof(double)));
+                if (tid == 0) bulk_s2g(dst, sQ, (unsigned)(n * sizeof(double)));
             } else {
-                for (int e = tid; e < n; e += NT) dst[e] = sA[e];
+                for (int e = tid; e < n; e += NT) dst[e] = sQ[e];
             }
-            qout_src = sA;
+            qout_src = sQ;
         }
     }
 
@@ -849,52 +870,30 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     if (!DIAG && a.t_out) {
         __syncthreads();
         R *to = reinterpret_cast<R *>(a.t_out);
-        // the output state: sA (double), or its float copy over the state
-        // slots (9 floats at the start of each point's 9 doubles)
-        constexpr int PS = sizeof(R) == sizeof(double) ? 9 : 18;  // R per point
-        const R *qo = sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(qout_src)
-                                                  : reinterpret_cast<const R *>(sQ);
-        if constexpr (sizeof(R) == sizeof(double)) {
-            // one thread per (cell, family, variable, line): the line's N
-            // values give the traces at both of its ends (r = 0 and r = N),
-            // each summed in order as phase A sums them (measured faster than
-            // one thread per face point in the FP64 forms, slower in the mixed)
-            for (int t = tid; t < ncl * 2 * 9 * N; t += NT) {
-                const int line = t % N, k = (t / N) % 9, fam = (t / (9 * N)) % 2, c = t / (18 * N);
-                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line) + k;
-                const int stride = fam == 0 ? PS : PS * N;
-                R qs[N];
+        // one thread per (cell, family, variable, line): the line's N output
+        // values (sQ, double, rounded once to the arithmetic type) give the
+        // traces at both of its ends (r = 0 and r = N), each summed in order
+        // as phase A sums them
+        for (int t = tid; t < ncl * 2 * 9 * N; t += NT) {
+            const int line = t % N, k = (t / N) % 9, fam = (t / (9 * N)) % 2, c = t / (18 * N);
+            const double *q = qout_src + c * NQ + (fam == 0 ? 9 * N * line : 9 * line) + k;
+            const int stride = fam == 0 ? 9 : 9 * N;
+            R qs[N];
 #pragma unroll
-                for (int s = 0; s < N; s++) qs[s] = q[stride * s];
-                R a0 = (R)0, aN = (R)0;
+            for (int s = 0; s < N; s++) qs[s] = (R)q[stride * s];
+            R a0 = (R)0, aN = (R)0;
 #pragma unroll
-                for (int s = 0; s < N; s++) {
-                    a0 = a0 + qs[s] * sOpL[s];
-                    aN = aN + qs[s] * sOpL[N * N + s];
-                }
-                // the faces at the line's ends (face_point inverted): xi line j
-                // ends on local faces 4 (point N-j) and 2 (point j+1), eta
-                // line i on local faces 1 (point i+1) and 3 (point N-i)
-                const int lf0 = fam == 0 ? 4 : 1, nfp0 = fam == 0 ? N - line : line + 1;
-                const int lfN = fam == 0 ? 2 : 3, nfpN = fam == 0 ? line + 1 : N - line;
-                to[trace_at<N>(c0 + c, lf0, nfp0 - 1, k)] = a0;
-                to[trace_at<N>(c0 + c, lfN, nfpN - 1, k)] = aN;
+            for (int s = 0; s < N; s++) {
+                a0 = a0 + qs[s] * sOpL[s];
+                aN = aN + qs[s] * sOpL[N * N + s];
             }
-        } else {
-            for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
-                const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
-                int fam, line, r;
-                face_point<N>(lf, nfp, fam, line, r);
-                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
-                const int stride = fam == 0 ? PS : PS * N;
-#pragma unroll
-                for (int k = 0; k < 9; k++) {
-                    R acc = (R)0;
-#pragma unroll
-                    for (int s = 0; s < N; s++) acc = acc + q[k + stride * s] * sOpL[r * N + s];
-                    to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
-                }
-            }
+            // the faces at the line's ends (face_point inverted): xi line j
+            // ends on local faces 4 (point N-j) and 2 (point j+1), eta line i
+            // on local faces 1 (point i+1) and 3 (point N-i)
+            const int lf0 = fam == 0 ? 4 : 1, nfp0 = fam == 0 ? N - line : line + 1;
+            const int lfN = fam == 0 ? 2 : 3, nfpN = fam == 0 ? line + 1 : N - line;
+            to[trace_at<N>(c0 + c, lf0, nfp0 - 1, k)] = a0;
+            to[trace_at<N>(c0 + c, lfN, nfpN - 1, k)] = aN;
         }
     }
 

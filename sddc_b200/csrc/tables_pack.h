@@ -73,14 +73,18 @@ struct FaceLists {
     int nfree;
     const int *cyc2fpair;
     int npair;
+    // processor faces of a decomposed run (IBFPROC, in exchange-slot order;
+    // IF2C(K,1) and IF2C(K,3) are the own cell and its local face)
+    const int *ibfproc = nullptr;
+    int nproc = 0;
 };
 
 // rec[2 * (cell * 4 + lf - 1) + {0, 1}] (cell 0-based): the partner cell
-// (0-based; -1 on a boundary) and kind | partner's local face << 8.  A shared
-// face (interior or cyclic pair) gives its left cell (IF2C(:,1), the first
-// face of a pair) kind kFaceLeft and the other kFaceRight.  Returns "" or
-// what is wrong with the lists (an entry out of range, a (cell, local face)
-// listed twice or in no list).
+// (0-based; -1 on a boundary; the exchange slot of a processor face) and
+// kind | partner's local face << 8.  A shared face (interior or cyclic pair)
+// gives its left cell (IF2C(:,1), the first face of a pair) kind kFaceLeft
+// and the other kFaceRight.  Returns "" or what is wrong with the lists (an
+// entry out of range, a (cell, local face) listed twice or in no list).
 inline std::string build_face_records(int ncell, const FaceLists &fl, int *rec)
 {
     for (size_t k = 0; k < (size_t)ncell * 4; k++) {
@@ -127,11 +131,19 @@ inline std::string build_face_records(int ncell, const FaceLists &fl, int *rec)
             if (!face_ok(f)) { msg = "boundary list entry out of range"; break; }
             claim(IF2(f, 1), IF2(f, 3), 0, kinds[t], 0);
         }
+    for (int b = 0; b < fl.nproc && msg.empty(); b++) {
+        const int f = fl.ibfproc[b];
+        if (!face_ok(f)) { msg = "IBFPROC entry out of range"; break; }
+        const int cell = IF2(f, 1), lf = IF2(f, 3);
+        claim(cell, lf, 0, kFaceProc, 0);
+        if (msg.empty()) rec[2 * ((size_t)(cell - 1) * 4 + (lf - 1))] = b;
+    }
     if (msg.empty())
         for (size_t k = 0; k < (size_t)ncell * 4; k++)
             if ((rec[2 * k + 1] & 0xff) == kFaceNone) {
                 msg = "cell " + std::to_string(k / 4 + 1) + " local face " + std::to_string(k % 4 + 1) +
-                      " is in no face list (processor faces do not exist on one GPU)";
+                      " is in no face list (a face whose other cell is on another rank is a processor face, "
+                      "sddc_set_proc_faces)";
                 break;
             }
     return msg;

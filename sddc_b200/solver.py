@@ -33,7 +33,8 @@ EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables",
             "sddc_compresid", "sddc_rk_step", "sddc_get_state", "sddc_monitor", "sddc_get_maxima",
             "sddc_state_device_ptr", "sddc_get_stream", "sddc_set_cases", "sddc_rk_step_cases",
             "sddc_get_case_maxima", "sddc_vjp_resid", "sddc_adjoint_run", "sddc_set_plot", "sddc_plot_nodes",
-            "sddc_write_tecplot", "sddc_write_restart", "sddc_output_wait")
+            "sddc_write_tecplot", "sddc_write_restart", "sddc_output_wait", "sddc_set_proc_faces",
+            "sddc_set_exchange")
 
 
 class Params(ctypes.Structure):
@@ -59,6 +60,10 @@ class AdjointStats(ctypes.Structure):
     """sddc_adjoint_stats."""
     _fields_ = [("forward_ms", _D), ("reverse_ms", _D), ("device_bytes", _D), ("owner_stages", _I),
                 ("tie_stages", _I)]
+
+
+# int (*sddc_exchange_fn)(void *user)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
 
 class SddcError(RuntimeError):
@@ -99,6 +104,9 @@ def lib():
         L.sddc_write_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.sddc_write_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _I, _PI]
         L.sddc_output_wait.argtypes = [ctypes.c_void_p]
+        L.sddc_set_proc_faces.argtypes = [ctypes.c_void_p, _I, _PI]
+        L.sddc_set_exchange.argtypes = [ctypes.c_void_p, EXCHANGE_FN, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p]
         L._sddc_typed = True
     return L
 
@@ -107,7 +115,10 @@ class Solver:
     """One case on the current GPU."""
 
     def __init__(self, tables, physics, precision="fp64", k_stage: int = 3, cells_per_cta: int = 0,
-                 ncellglob: int | None = None):
+                 ncellglob: int | None = None, proc_faces=None):
+        """proc_faces: the processor faces of one partition of a decomposed
+        run (local face ids, 1-based, in exchange-slot order; see
+        partition.Part); the exchange follows with set_exchange."""
         self.N = tables.N
         self.ncell = tables.ncell
         self.tables = tables
@@ -128,6 +139,10 @@ class Solver:
             raise SddcError(rc, msg)
         t = tables
         keep = []
+        if proc_faces is not None:
+            pf = np.ascontiguousarray(proc_faces, dtype=np.int32)
+            keep.append(pf)
+            self._check(self._L.sddc_set_proc_faces(self._h, int(pf.shape[0]), ptr(pf, _I)))
 
         def ia(a):
             a = np.asfortranarray(a, dtype=np.int32)
@@ -221,6 +236,26 @@ class Solver:
         p = ctypes.c_void_p()
         self._check(self._L.sddc_get_stream(self._h, ctypes.byref(p)))
         return p.value
+
+    # -- decomposed runs -----------------------------------------------------
+    def set_exchange(self, fn, send_ptr: int, recv_ptr: int, maxima_ptr: int):
+        """fn(user) -> int is called between stages, on the context's stream,
+        after the library wrote this rank's processor-face traces to the
+        device buffer at send_ptr and its running maxima to maxima_ptr; it
+        exchanges the traces into recv_ptr and reduces the maxima (MAX) in
+        place, and returns 0."""
+        def tramp(user):
+            try:
+                return int(fn(user) or 0)
+            except Exception:  # an exception cannot cross into C
+                import traceback
+
+                traceback.print_exc()
+                return 1
+
+        self._exchange_cb = EXCHANGE_FN(tramp)  # kept alive with the solver
+        self._check(self._L.sddc_set_exchange(self._h, self._exchange_cb, None, ctypes.c_void_p(send_ptr),
+                                              ctypes.c_void_p(recv_ptr), ctypes.c_void_p(maxima_ptr)))
 
     # -- batches of cases ---------------------------------------------------
     def set_cases(self, records):

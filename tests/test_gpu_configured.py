@@ -29,10 +29,17 @@ from sddc_b200.solver import NumericalFault, Solver
 pytestmark = pytest.mark.gpu
 
 NAMES = ["rho", "rhou", "rhov", "rhow", "E", "Bx", "By", "Bz", "psi"]
-# mixed form against the oracle after the 89 steps to t = 0.5 on 32 x 32:
-# per variable (relative to that variable's norm) and over all nine
-MIXED_OT_T05_PER_VAR = 2e-6
-MIXED_OT_T05_ALL = 1e-6
+# Mixed form against the oracle after the 89 steps to t = 0.5 on 32 x 32
+# (measured: 1.0e-7 over all nine variables; per variable at most 6.1e-8
+# relative to the whole state's norm, at most 2.1e-7 relative to the
+# variable's own norm, except psi).  psi, the GLM cleaning field, stays
+# near zero: the FP32 div B source perturbs it by ~1e-8 of the state's
+# scale, which is 2.8e-4 of its own norm at 32 x 32 (and grows as the mesh
+# refines); it is held to its own bar.
+MIXED_OT_T05_ALL = 3e-7
+MIXED_OT_T05_STATE_SCALE = 2e-7
+MIXED_OT_T05_OWN = 6e-7
+MIXED_OT_T05_PSI_OWN = 1e-3
 
 
 @pytest.fixture(scope="module")
@@ -97,13 +104,13 @@ def test_orszag_tang_mixed_to_t05(ot32):
     s.set_state(ot32["Q0"])
     s.rk_s5p3(ot32["dt"], ot32["nsteps"])
     q, ref = s.state()["Q"], ot32["end"]["Q"]
-    errs = {n: rel_l2(q[k], ref[k]) for k, n in enumerate(NAMES) if n not in ("rhow", "Bz")}
-    # rho w and Bz stay at the 1e-8 noise level (the vortex is planar), so
-    # their own norms are no scale; they are held to the state's scale
-    for k in (3, 7):
-        errs[NAMES[k]] = float(np.linalg.norm(q[k] - ref[k]) / np.linalg.norm(ref))
-    assert max(errs.values()) <= MIXED_OT_T05_PER_VAR, errs
+    scale = np.linalg.norm(ref)
+    state_scale = {n: float(np.linalg.norm(q[k] - ref[k]) / scale) for k, n in enumerate(NAMES)}
+    own = {n: rel_l2(q[k], ref[k]) for k, n in enumerate(NAMES)}
     assert rel_l2(q, ref) <= MIXED_OT_T05_ALL
+    assert max(state_scale.values()) <= MIXED_OT_T05_STATE_SCALE, state_scale
+    assert max(v for n, v in own.items() if n != "psi") <= MIXED_OT_T05_OWN, own
+    assert own["psi"] <= MIXED_OT_T05_PSI_OWN, own
     s.close()
 
 
