@@ -228,6 +228,11 @@ int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases);
 int sddc_rk_step_cases(sddc_ctx *ctx, int nsteps);
 /* Running maxima of one case after the last evaluation. */
 int sddc_get_case_maxima(sddc_ctx *ctx, int icase, double *eigvmax, double *umax);
+/* How a batch's stages launch: on != 0, each stage is one persistent
+   launch of as many CTAs as are resident at once, each walking the tile
+   table (largest case first) with a grid stride; 0 (the default), one CTA
+   per tile.  No counterpart in the reference (it runs one case per job). */
+int sddc_set_persistent(sddc_ctx *ctx, int on);
 
 /* ---- residual evaluation without device allocation ----------------------
    No counterpart in the reference.  For callers that cannot call cudaMalloc:

@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -548,6 +549,7 @@ static cudaError_t launch(sddc_ctx *ctx, bool diag, const StageArgs &a_in)
         a.tiles = diag ? ctx->tiles_diag : ctx->tiles_rk;
         a.ntiles = diag ? ctx->ntiles_diag : ctx->ntiles_rk;
         a.cases = ctx->case_dev;
+        a.persistent = ctx->persistent ? 1 : 0;
     }
     switch (ctx->p.precision) {
     case SDDC_FP64_EXACT: return launch_stage_exact(ctx->N, ctx->cpb, diag, a, ctx->ops, ctx->stream);
@@ -876,8 +878,15 @@ extern "C" int sddc_get_stream(sddc_ctx *ctx, void **stream)
 
 static int build_tiles(sddc_ctx *ctx, int cpb, int4 **dev, int *count)
 {
+    // persistent launches walk the table with a grid stride, largest case
+    // first; otherwise the cases in their order
+    std::vector<int> order(ctx->ncase);
+    for (int c = 0; c < ctx->ncase; c++) order[c] = c;
+    if (ctx->persistent)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return ctx->cases[x].ncell > ctx->cases[y].ncell; });
     std::vector<int4> tiles;
-    for (int c = 0; c < ctx->ncase; c++) {
+    for (int c : order) {
         const sddc_case &k = ctx->cases[c];
         for (int first = 0; first < k.ncell; first += cpb)
             tiles.push_back(make_int4(k.first_cell + first, std::min(cpb, k.ncell - first), c, first == 0 ? 1 : 0));
@@ -940,6 +949,25 @@ extern "C" int sddc_set_cases(sddc_ctx *ctx, int ncase, const sddc_case *cases)
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->state = false;  // the maxima were reset: set the state again
     ctx->mon_nblk = 0;
+    return SDDC_OK;
+}
+
+extern "C" int sddc_set_persistent(sddc_ctx *ctx, int on)
+{
+    if (!ctx) return SDDC_EINVAL;
+    ctx->persistent = on != 0;
+    if (ctx->ncase) {  // the tile tables in the launch's order
+        int rc;
+        if ((rc = build_tiles(ctx, ctx->cpb, &ctx->tiles_rk, &ctx->ntiles_rk)) ||
+            (rc = build_tiles(ctx, 8, &ctx->tiles_diag, &ctx->ntiles_diag)))
+            return rc;
+    }
+    for (auto &g : ctx->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    CK(cudaStreamSynchronize(ctx->stream));
     return SDDC_OK;
 }
 

@@ -96,6 +96,7 @@ struct sddc_ctx {
     CaseParams *case_dev = nullptr;
     int4 *tiles_rk = nullptr, *tiles_diag = nullptr;
     int ntiles_rk = 0, ntiles_diag = 0;
+    bool persistent = false;  // batch stages as grid-stride persistent launches
     // discrete adjoint work space (adjoint.cu), created on first use
     sddc::AdjWs *adj = nullptr;
     // viscous / resistive chain (vismode = 1 with mu or eta0 nonzero)

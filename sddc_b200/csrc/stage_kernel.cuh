@@ -87,6 +87,9 @@ struct StageArgs {
     // a single case
     const int4 *tiles;
     int ntiles;
+    // batch launched persistently: each CTA walks the tile table with a grid
+    // stride (the table is ordered largest case first); 0: one CTA per tile
+    int persistent;
     const CaseParams *cases;
     const double *__restrict__ q_in;   // (9,N,N,NCELL), never written during the stage
     double *q_out;                     // RK output (may be reg_a: FiveStageRk stage 5)
@@ -138,6 +141,10 @@ __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned coun
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
 {
@@ -248,10 +255,9 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_bytes()
 {
     using S = Smem<N, R, DIAG>;
-    // sQ and sJac; the residual staging sA and the sensor's sJz and sLow in
-    // residual evaluations only (a time step forms its output over sQ)
-    size_t d = (size_t)CPB * ((DIAG ? 2 : 1) * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) +
-               4 * 32 + 2 * (N - 1) * N;
+    // sQ, sA, sJac; the sensor's sJz and sLow in residual evaluations only
+    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) + 4 * 32 +
+               2 * (N - 1) * N;
     size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam) + 2 * (N + 1) * N;
     return d * sizeof(double) + r * sizeof(R);
 }
@@ -267,11 +273,12 @@ template <int N, int CPB, typename R, bool DIAG> constexpr int stage_min_blocks(
     return b;
 }
 
+// One tile (CPB consecutive cells, or an entry of a batch's tile table) by
+// the whole CTA; false if the staging copies timed out (the CTA stops).
 // EXACT instantiations are compiled without FMA contraction (-fmad=false) in
 // their own translation unit; they reproduce the reference's FP64 rounding.
 template <int N, int CPB, typename R, bool DIAG, bool EXACT>
-__global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
-    stage_kernel(const StageArgs a, const Ops ops)
+__device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, const int tile)
 {
     constexpr bool EX = EXACT && (sizeof(R) == sizeof(double));
     // a time step of the forms other than the exact one needs only div B:
@@ -294,8 +301,9 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     double *sJz = sJac + CPB * NJ;                               // [CPB][NN]  Jz^2 for the sensor (DIAG)
     double *sLow = sJz + (DIAG ? CPB * NN : 0);                  // [CPB][kLow] (DIAG)
     double *sRed = sLow + (DIAG ? CPB * S::kLow : 0);            // [4][32] block reductions
-    double *sA = sRed + 4 * 32;                                  // [CPB][NQ] residual (DIAG only)
-    double *sOpH = sA + (DIAG ? CPB * NQ : 0);                   // [N-1][N]  AV projection
+    // residual (DIAG); in a time step the RK register, then the output
+    double *sA = sRed + 4 * 32;                                  // [CPB][NQ]
+    double *sOpH = sA + CPB * NQ;                                // [N-1][N]  AV projection
     double *sOpHL = sOpH + (N - 1) * N;                          // [N][N-1]  AV prolongation
     R *sNrm = reinterpret_cast<R *>(sOpHL + N * (N - 1));        // [CPB][NM] flux-point normals
     R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
@@ -309,16 +317,16 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     int c0, ncl, cs;
     bool first_tile;
     if (a.tiles) {
-        const int4 tl = a.tiles[blockIdx.x];
+        const int4 tl = a.tiles[tile];
         c0 = tl.x;
         ncl = tl.y;
         cs = tl.z;
         first_tile = tl.w != 0;
     } else {
-        c0 = blockIdx.x * CPB;
+        c0 = tile * CPB;
         ncl = min(CPB, a.ncell - c0);  // cells of this CTA
         cs = 0;
-        first_tile = blockIdx.x == 0;
+        first_tile = tile == 0;
     }
     // per-case data is read where it is used (kept out of registers)
     double *maxima = a.maxima + 10 * cs;
@@ -326,10 +334,10 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     // ---- stage the state, the metrics and the operators ------------------------
     // The tile's state slice goes to sQ, its normals to sNrm and Jac to sJac
     // (or, without the split metric arrays, its packed metric records to the
-    // flux buffer, free until phase A, for conversion) by TMA bulk copies that
-    // one thread issues when every slice is 16-byte aligned; otherwise by
-    // batches of loads.  In a stage that reads one RK register, that
-    // register's slice is brought into L2 now and read by phase C's threads.
+    // flux buffer, free until phase A, for conversion) and, in a stage that
+    // reads one RK register, that register's slice to sA, by TMA bulk copies
+    // that one thread issues when every slice is 16-byte aligned; otherwise
+    // by batches of loads.
     __shared__ __align__(8) unsigned long long sBar;
     __shared__ int sAbort;
     double *sMetRaw = reinterpret_cast<double *>(sF);
@@ -346,12 +354,13 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     const double *rsrc = want_ra ? a.reg_a + (size_t)c0 * NQ : nullptr;
     const bool bulk = ((uintptr_t)qsrc & 15) == 0 && (qbytes & 15) == 0 &&
                       (split ? (((uintptr_t)nsrc | (uintptr_t)jsrc | nbytes | jbytes) & 15) == 0
-                             : (((uintptr_t)msrc0 | mbytes) & 15) == 0);  // uniform in the CTA
+                             : (((uintptr_t)msrc0 | mbytes) & 15) == 0) &&
+                      (!want_ra || ((uintptr_t)rsrc & 15) == 0);  // uniform in the CTA
     if (tid == 0) {
         sAbort = 0;
         if (bulk) {
             mbar_init(&sBar, 1);
-            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes));
+            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes + (want_ra ? qbytes : 0)));
             bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
             if (split) {
                 bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
@@ -359,8 +368,8 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             } else {
                 bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
             }
+            if (want_ra) bulk_g2s(sA, rsrc, (unsigned)qbytes, &sBar);
         }
-        if (want_ra && ((uintptr_t)rsrc & 15) == 0 && (qbytes & 15) == 0) bulk_prefetch_l2(rsrc, (unsigned)qbytes);
     }
     for (int k = tid; k < NP * N; k += NT) {
         sOpL[k] = opL<R>(ops, k);
@@ -391,6 +400,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         } else {
             stage_copy(sMetRaw, msrc0, ncl * ML::kSize);
         }
+        if (want_ra) stage_copy(sA, rsrc, ncl * NQ);
     }
     const double eig_r = maxima[2 * a.slot_r], um_r = maxima[2 * a.slot_r + 1];
     // compflux.f90:6 -- running maxima of all previous stages
@@ -403,7 +413,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         mbar_wait_bounded(&sBar, 0);
     }
     __syncthreads();
-    if (sAbort) return;
+    if (sAbort) return false;
     if (!split) {
         // the metric record: normals (rounded once to the arithmetic type) and Jac
         for (int k = tid; k < ncl * ML::kSize; k += NT) {
@@ -710,53 +720,43 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             for (int k = 0; k < 9; k++) part_r += res[k] * res[k];
             part_d += divB * divB;
         }
+        double *ap = sA + c * NQ + 9 * (i + N * j);
         if constexpr (DIAG) {
             // stage the residual for phase E's copy-out
-            double *ap = sA + c * NQ + 9 * (i + N * j);
 #pragma unroll
             for (int k = 0; k < 9; k++) ap[k] = res[k];
         } else {
-            // in a time step the residual goes, in the arithmetic type, over
-            // this point's xi-derivative slot (slot i of xi-line j), which no
-            // other thread reads; phase E takes it from there
-            R *rp = sF + c * S::kF + (0 * N + j) * NP * 9 + i * 9;
+            // ---- E: the RK stage update of this point (iterations.f90:88-213);
+            // the point's state and RK register slot are read by this thread
+            // only, so the output goes to the register slot in place, and in
+            // the float form a float copy over the state slot for phase F
+            // element by element in order: float copy k overwrites bytes of
+            // state element k/2 <= k, already read
+            const size_t g = (size_t)cell * NQ + 9 * (i + N * j);
+            const int kind = a.rk_kind;
+            R *qf = reinterpret_cast<R *>(sQ + c * NQ + 9 * (i + N * j));
 #pragma unroll
-            for (int k = 0; k < 9; k++) rp[k] = (R)res[k];
+            for (int k = 0; k < 9; k++) {
+                const double qk = q[k], r = res[k];
+                double o;
+                switch (kind) {
+                case kRkAxpy: o = qk + cf[0] * r; break;
+                case kRkTwoReg: o = (cf[1] * ap[k] + cf[2] * qk) + cf[0] * r; break;
+                case kRkTwoRegT: o = (cf[1] * ap[k] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
+                default:
+                    o = ((((cf[1] * a.reg_a[g + k] + cf[2] * a.reg_b[g + k]) + cf[3] * a.reg_c[g + k]) + cf[4] * qk) +
+                         cf[5] * a.reg_d[g + k]) +
+                        cf[0] * r;
+                    break;
+                }
+                ap[k] = o;
+                if (a.resid_w) a.resid_w[g + k] = r;
+                if constexpr (sizeof(R) != sizeof(double)) qf[k] = (R)o;
+            }
+            fence_proxy_async();  // sA is the source of the bulk store below
         }
     }
     __syncthreads();
-
-    // ---- E: the RK stage update (iterations.f90:88-213), element by element -----
-    // over the tile's slice: the state element (sQ), the residual (its point's
-    // xi-derivative slot) and the RK registers the stage reads (consecutive
-    // threads read consecutive register elements); the output goes over the
-    // state element in sQ, the source of the bulk store and of phase F
-    if constexpr (!DIAG) {
-        const size_t g0 = (size_t)c0 * NQ;
-        const int kind = a.rk_kind;
-        for (int e = tid; e < ncl * NQ; e += NT) {
-            const int k = e % 9, pt = e / 9;  // pt = c * NN + i + N * j
-            const int c = pt / NN, ij = pt - c * NN, i = ij % N, j = ij / N;
-            const double qk = sQ[e];
-            const double r = (double)sF[c * S::kF + (0 * N + j) * NP * 9 + i * 9 + k];
-            const size_t g = g0 + e;
-            double o;
-            switch (kind) {
-            case kRkAxpy: o = qk + cf[0] * r; break;
-            case kRkTwoReg: o = (cf[1] * a.reg_a[g] + cf[2] * qk) + cf[0] * r; break;
-            case kRkTwoRegT: o = (cf[1] * a.reg_a[g] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
-            default:
-                o = ((((cf[1] * a.reg_a[g] + cf[2] * a.reg_b[g]) + cf[3] * a.reg_c[g]) + cf[4] * qk) +
-                     cf[5] * a.reg_d[g]) +
-                    cf[0] * r;
-                break;
-            }
-            sQ[e] = o;
-            if (a.resid_w) a.resid_w[g] = r;
-        }
-        fence_proxy_async();  // sQ is the source of the bulk store below
-        __syncthreads();
-    }
 
     // ---- D: AV smoothness sensor (comp_artificial_viscosity, AV.f90:14-83) ------
     const bool av = DIAG && a.artiv == 1 && a.vismode == 1;
@@ -842,7 +842,7 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
         }
     }
 
-    // ---- residual copy-out (residual evaluation) or the output store ----------
+    // ---- E: residual copy-out (residual evaluation) or the output store ---------
     const double *qout_src = nullptr;
     bool out_bulk = false;
     {
@@ -852,17 +852,17 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
             if (a.resid_out)
                 for (int e = tid; e < n; e += NT) a.resid_out[g0 + e] = sA[e];
         } else {
-            // the output slice (formed over sQ by phase E) to q_out: one bulk
+            // the output slice (formed in sA by phase C) to q_out: one bulk
             // store issued by one thread, read from shared memory while phase
             // F runs, or coalesced stores when the slice is not 16-byte aligned
             double *dst = a.q_out + g0;
             out_bulk = (((uintptr_t)dst | (size_t)n * sizeof(double)) & 15) == 0;
             if (out_bulk) {
-                if (tid == 0) bulk_s2g(dst, sQ, (unsigned)(n * sizeof(double)));
+                if (tid == 0) bulk_s2g(dst, sA, (unsigned)(n * sizeof(double)));
             } else {
-                for (int e = tid; e < n; e += NT) dst[e] = sQ[e];
+                for (int e = tid; e < n; e += NT) dst[e] = sA[e];
             }
-            qout_src = sQ;
+            qout_src = sA;
         }
     }
 
@@ -870,30 +870,52 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
     if (!DIAG && a.t_out) {
         __syncthreads();
         R *to = reinterpret_cast<R *>(a.t_out);
-        // one thread per (cell, family, variable, line): the line's N output
-        // values (sQ, double, rounded once to the arithmetic type) give the
-        // traces at both of its ends (r = 0 and r = N), each summed in order
-        // as phase A sums them
-        for (int t = tid; t < ncl * 2 * 9 * N; t += NT) {
-            const int line = t % N, k = (t / N) % 9, fam = (t / (9 * N)) % 2, c = t / (18 * N);
-            const double *q = qout_src + c * NQ + (fam == 0 ? 9 * N * line : 9 * line) + k;
-            const int stride = fam == 0 ? 9 : 9 * N;
-            R qs[N];
+        // the output state: sA (double), or its float copy over the state
+        // slots (9 floats at the start of each point's 9 doubles)
+        constexpr int PS = sizeof(R) == sizeof(double) ? 9 : 18;  // R per point
+        const R *qo = sizeof(R) == sizeof(double) ? reinterpret_cast<const R *>(qout_src)
+                                                  : reinterpret_cast<const R *>(sQ);
+        if constexpr (sizeof(R) == sizeof(double)) {
+            // one thread per (cell, family, variable, line): the line's N
+            // values give the traces at both of its ends (r = 0 and r = N),
+            // each summed in order as phase A sums them (measured faster than
+            // one thread per face point in the FP64 forms, slower in the mixed)
+            for (int t = tid; t < ncl * 2 * 9 * N; t += NT) {
+                const int line = t % N, k = (t / N) % 9, fam = (t / (9 * N)) % 2, c = t / (18 * N);
+                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line) + k;
+                const int stride = fam == 0 ? PS : PS * N;
+                R qs[N];
 #pragma unroll
-            for (int s = 0; s < N; s++) qs[s] = (R)q[stride * s];
-            R a0 = (R)0, aN = (R)0;
+                for (int s = 0; s < N; s++) qs[s] = q[stride * s];
+                R a0 = (R)0, aN = (R)0;
 #pragma unroll
-            for (int s = 0; s < N; s++) {
-                a0 = a0 + qs[s] * sOpL[s];
-                aN = aN + qs[s] * sOpL[N * N + s];
+                for (int s = 0; s < N; s++) {
+                    a0 = a0 + qs[s] * sOpL[s];
+                    aN = aN + qs[s] * sOpL[N * N + s];
+                }
+                // the faces at the line's ends (face_point inverted): xi line j
+                // ends on local faces 4 (point N-j) and 2 (point j+1), eta
+                // line i on local faces 1 (point i+1) and 3 (point N-i)
+                const int lf0 = fam == 0 ? 4 : 1, nfp0 = fam == 0 ? N - line : line + 1;
+                const int lfN = fam == 0 ? 2 : 3, nfpN = fam == 0 ? line + 1 : N - line;
+                to[trace_at<N>(c0 + c, lf0, nfp0 - 1, k)] = a0;
+                to[trace_at<N>(c0 + c, lfN, nfpN - 1, k)] = aN;
             }
-            // the faces at the line's ends (face_point inverted): xi line j
-            // ends on local faces 4 (point N-j) and 2 (point j+1), eta line i
-            // on local faces 1 (point i+1) and 3 (point N-i)
-            const int lf0 = fam == 0 ? 4 : 1, nfp0 = fam == 0 ? N - line : line + 1;
-            const int lfN = fam == 0 ? 2 : 3, nfpN = fam == 0 ? line + 1 : N - line;
-            to[trace_at<N>(c0 + c, lf0, nfp0 - 1, k)] = a0;
-            to[trace_at<N>(c0 + c, lfN, nfpN - 1, k)] = aN;
+        } else {
+            for (int t = tid; t < ncl * 4 * N; t += NT) {  // one thread per face point
+                const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
+                int fam, line, r;
+                face_point<N>(lf, nfp, fam, line, r);
+                const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
+                const int stride = fam == 0 ? PS : PS * N;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    R acc = (R)0;
+#pragma unroll
+                    for (int s = 0; s < N; s++) acc = acc + q[k + stride * s] * sOpL[r * N + s];
+                    to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
+                }
+            }
         }
     }
 
@@ -931,16 +953,33 @@ __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CP
                 atomic_max_nonneg(&maxima[2 * a.slot_w + 1], um_r);
             }
             if (a.mon_part) {
-                a.mon_part[2 * blockIdx.x] = s0;
-                a.mon_part[2 * blockIdx.x + 1] = s1;
+                a.mon_part[2 * tile] = s0;
+                a.mon_part[2 * tile + 1] = s1;
             }
             if (a.cta_max) {  // where the running maxima were raised (the adjoint's argmax)
-                a.cta_max[2 * blockIdx.x] = m0;
-                a.cta_max[2 * blockIdx.x + 1] = m1;
+                a.cta_max[2 * tile] = m0;
+                a.cta_max[2 * tile + 1] = m1;
             }
-            // the bulk store must have read sA before the CTA's shared memory goes
+            // the bulk store must have read sA before the CTA's shared memory
+            // goes or the next tile reuses it; the staging barrier is free
             if (out_bulk) bulk_wait_read();
+            if (bulk) mbar_inval(&sBar);
         }
+    }
+    return true;
+}
+
+template <int N, int CPB, typename R, bool DIAG, bool EXACT>
+__global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
+    stage_kernel(const StageArgs a, const Ops ops)
+{
+    if (a.tiles && a.persistent) {
+        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+            if (!stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, t)) return;
+            __syncthreads();  // tile t's last shared-memory reads before tile t+grid stages
+        }
+    } else {
+        stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, blockIdx.x);
     }
 }
 

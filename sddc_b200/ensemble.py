@@ -92,9 +92,11 @@ class Member:
 
 
 class Batch:
-    """All members stepped together by one context (one launch per stage)."""
+    """All members stepped together by one context: one launch per stage,
+    either one CTA per tile or (persistent=True) as many CTAs as are resident,
+    each walking the tile table largest case first."""
 
-    def __init__(self, members, precision="mixed", cells_per_cta=0):
+    def __init__(self, members, precision="mixed", cells_per_cta=0, persistent=False):
         self.members = members
         merged, first = merge([m.tables for m in members])
         for m, f in zip(members, first):
@@ -107,6 +109,8 @@ class Batch:
             recs.append(dict(first_cell=m.first_cell, ncell=m.tables.ncell, dt=m.dt, rinf=ph.rinf, pinf=ph.pinf,
                              uinf=ph.uinf, vinf=ph.vinf, bxinf=ph.bxinf, byinf=ph.byinf))
         self.solver.set_cases(recs)
+        if persistent:
+            self.solver.set_persistent(True)
         self.Q0 = np.asfortranarray(np.concatenate([m.Q0 for m in members], axis=-1))
 
     @property

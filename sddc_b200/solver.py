@@ -34,7 +34,7 @@ EXPORTED = ("sddc_create", "sddc_destroy", "sddc_last_error", "sddc_set_tables",
             "sddc_state_device_ptr", "sddc_get_stream", "sddc_set_cases", "sddc_rk_step_cases",
             "sddc_get_case_maxima", "sddc_vjp_resid", "sddc_adjoint_run", "sddc_set_plot", "sddc_plot_nodes",
             "sddc_write_tecplot", "sddc_write_restart", "sddc_output_wait", "sddc_set_proc_faces",
-            "sddc_set_exchange")
+            "sddc_set_exchange", "sddc_set_persistent")
 
 
 class Params(ctypes.Structure):
@@ -105,6 +105,7 @@ def lib():
         L.sddc_write_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _I, _PI]
         L.sddc_output_wait.argtypes = [ctypes.c_void_p]
         L.sddc_set_proc_faces.argtypes = [ctypes.c_void_p, _I, _PI]
+        L.sddc_set_persistent.argtypes = [ctypes.c_void_p, _I]
         L.sddc_set_exchange.argtypes = [ctypes.c_void_p, EXCHANGE_FN, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p]
         L._sddc_typed = True
@@ -267,6 +268,11 @@ class Solver:
                 setattr(arr[k], f, r[f])
         self._check(self._L.sddc_set_cases(self._h, len(records), arr))
         self.ncase = len(records)
+
+    def set_persistent(self, on=True):
+        """Batch stages as persistent grid-stride launches (largest case
+        first) instead of one CTA per tile."""
+        self._check(self._L.sddc_set_persistent(self._h, int(bool(on))))
 
     def step_cases(self, nsteps=1):
         self._check(self._L.sddc_rk_step_cases(self._h, int(nsteps)))

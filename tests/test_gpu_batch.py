@@ -14,12 +14,23 @@ def _members():
     return ensemble.build_members(cl)
 
 
+def _large_members():
+    """More tiles than CTAs are resident at once, so that persistent CTAs
+    walk several tiles; one case size not a multiple of the tile."""
+    cl = [cases.cylinder_case(64, 128, 4, ms=0.25, ma=2.0, seed=4, noise=1e-4),
+          cases.cylinder_case(9, 10, 4, ms=0.3, ma=4.0, seed=5, noise=1e-4),
+          cases.cylinder_case(60, 100, 4, ms=0.2, ma=1.5, seed=6, noise=1e-4),
+          cases.cylinder_case(48, 96, 4, ms=0.22, ma=3.0, seed=7, noise=1e-4)]
+    return ensemble.build_members(cl)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "mixed"])
 @pytest.mark.parametrize("cpb", [4, 8])
-def test_batch_equals_separate_runs(precision, cpb):
-    members = _members()
-    b = ensemble.Batch(members, precision=precision, cells_per_cta=cpb)
+@pytest.mark.parametrize("persistent", [False, True])
+def test_batch_equals_separate_runs(precision, cpb, persistent):
+    members = _members() if not persistent else _large_members()
+    b = ensemble.Batch(members, precision=precision, cells_per_cta=cpb, persistent=persistent)
     b.reset()
     b.step(3)
     Qb = b.solver.state()["Q"]
