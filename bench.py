@@ -380,13 +380,15 @@ def accuracy_run(solver_mod, t, ph, Q0, dt, dof, nsteps):
     return res
 
 
-def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200):
+def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200, max_steps=0, forms=("fp64_exact", "fp64", "mixed")):
     """The Orszag-Tang vortex on a periodic 1024^2 mesh, p = 3, to t = 0.5
     (dt fixed from CFL 0.3 of the initial state): each form from the same
     seeded initial state, its DOF-stage/s (CUDA events on the context's
     stream), and the mixed and FP64 forms' error against the exact FP64 form
     (bit-equal to the CPU oracle) at the end: per-variable rel-L2, ||divB||,
-    mass drift.  A form that faults numerically reports the time reached."""
+    mass drift.  A form that faults numerically reports the time reached.
+    max_steps > 0 stops after that many steps (the short runs profiled under
+    ncu); forms selects the forms run."""
     from sddc_b200 import cases, host
     from sddc_b200.solver import NumericalFault, Solver
 
@@ -395,10 +397,12 @@ def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200):
     Q0 = c.initial_state(t)
     dt = cases.cfl_dt(c.mesh, Q0, c.N)
     nsteps = int(math.ceil(t_end / dt))
+    if max_steps:
+        nsteps = min(nsteps, max_steps)
     dof = c.mesh.ncell * c.N * c.N
     out, res = {}, {"workload": f"Orszag-Tang {n}x{n} periodic, p=3 (N=4), RK_S5P3, CFL 0.3, t_end={t_end}",
                     "dof": dof, "dt": dt, "steps": nsteps}
-    for prec in ("fp64_exact", "fp64", "mixed"):
+    for prec in forms:
         s = Solver(t, c.physics, precision=prec)
         s.set_state(Q0)
         m0 = s.monitor()["mass"]
@@ -422,13 +426,13 @@ def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200):
         res[prec] = {"steps_done": done, "t_reached": done * dt, "fault": fault,
                      "value": dof * 5 * done / (ms / 1e3) if ms > 0 else None, "unit": UNIT}
         s.close()
-    ref, m0, mref = out["fp64_exact"]
+    ref, m0, mref = out.get("fp64_exact", (None, None, None))
     names = ["rho", "rhou", "rhov", "rhow", "E", "Bx", "By", "Bz", "psi"]
     if ref is not None:
         res["fp64_exact"].update(divB_l2=float(np.sqrt(mref["divbsum"] / dof)),
                                  mass_change=(mref["mass"] - m0) / m0)
         for prec in ("fp64", "mixed"):
-            q, m0p, mon = out[prec]
+            q, m0p, mon = out.get(prec, (None, None, None))
             if q is None:
                 continue
             res[prec].update(
@@ -462,7 +466,7 @@ def ensemble_run(torch, ncase=64, steps=1000, warmup=3, seed=0):
 
     # tile for the batch (untimed tuning on the batch itself)
     best, best_t = 4, None
-    for cpb in (4, 8, 16):
+    for cpb in autotune.CANDIDATES:
         b = ensemble.Batch(members, precision="mixed", cells_per_cta=cpb)
         b.reset()
         b.step(2)
@@ -747,12 +751,14 @@ def main():
                     help="RK3 steps of the mixed/FP64 vs FP64-exact comparison (0: skip)")
     ap.add_argument("--adjoint-steps", type=int, default=1200,
                     help="RK3 steps of the discrete-adjoint block (objective over the last sixth; 0: skip)")
-    ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8, 16],
+    ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 6, 8, 16],
                     help="cells per CTA; 0 lets the autotuner choose")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the discrete-adjoint block (with --adjoint-steps; the command profiled under ncu)")
     ap.add_argument("--orszag-tang", action="store_true",
                     help="run only the Orszag-Tang 1024^2 comparison (mixed/FP64 vs exact FP64 to t = 0.5)")
+    ap.add_argument("--ot-n", type=int, default=1024, help="Orszag-Tang cells per side")
+    ap.add_argument("--ot-steps", type=int, default=0, help="Orszag-Tang: stop after this many steps (0: t = 0.5)")
     args = ap.parse_args()
     global FIXED_TILE
     FIXED_TILE = args.tile
@@ -768,7 +774,8 @@ def main():
     if args.orszag_tang:
         import torch
 
-        print(json.dumps({"orszag_tang": orszag_tang_run(torch)}))
+        forms = (args.only,) if args.only else ("fp64_exact", "fp64", "mixed")
+        print(json.dumps({"orszag_tang": orszag_tang_run(torch, n=args.ot_n, max_steps=args.ot_steps, forms=forms)}))
         return
     if args.impl == "reference":
         run_reference(args)

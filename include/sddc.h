@@ -60,7 +60,7 @@ typedef struct sddc_params {
     int artiv;      /* ARTIV: 1 computes the AV sensor                         */
     int k_stage;    /* 3: RK_S5P3, 5: FiveStageRk                              */
     int precision;  /* SDDC_FP64_EXACT, SDDC_FP64 or SDDC_MIXED                */
-    int cells_per_cta; /* 0: default tile; else 4, 8 or 16 cells per CTA       */
+    int cells_per_cta; /* 0: default tile; else 4, 6, 8 or 16 cells per CTA    */
     double mu, eta0;   /* viscosity and resistivity (QUAD.INP), >= 0            */
     double dxcycl, dycycl;
     double rinf, pinf, uinf, vinf, bxinf, byinf; /* free stream (QUAD.INP) */

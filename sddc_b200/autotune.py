@@ -17,7 +17,7 @@ import time
 from . import _native
 from .solver import Solver
 
-CANDIDATES = (4, 8, 16)
+CANDIDATES = (4, 6, 8, 16)
 CACHE = os.path.join(_native.LIB_DIR, "autotune.json")
 
 

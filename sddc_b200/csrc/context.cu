@@ -203,8 +203,9 @@ extern "C" int sddc_create(sddc_ctx **out, const sddc_params *p)
     if (p->k_stage != 3 && p->k_stage != 5) return bad("k_stage can be only 3 or 5 (iterations.f90:22-31)");
     if (p->precision < SDDC_FP64_EXACT || p->precision > SDDC_MIXED) return bad("unknown precision");
     if (!(p->mu >= 0.0) || !(p->eta0 >= 0.0)) return bad("mu and eta0 must be non-negative");
-    if (p->cells_per_cta != 0 && p->cells_per_cta != 4 && p->cells_per_cta != 8 && p->cells_per_cta != 16)
-        return bad("cells_per_cta must be 0, 4, 8 or 16");
+    if (p->cells_per_cta != 0 && p->cells_per_cta != 4 && p->cells_per_cta != 6 && p->cells_per_cta != 8 &&
+        p->cells_per_cta != 16)
+        return bad("cells_per_cta must be 0, 4, 6, 8 or 16");
     ctx->N = p->N;
     ctx->ncell = p->ncell;
     ctx->cpb = p->cells_per_cta ? p->cells_per_cta : 8;

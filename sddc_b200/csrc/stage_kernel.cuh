@@ -39,9 +39,13 @@ namespace sddc {
 
 constexpr int kMaxN = 6;
 
-// threads of a CTA owning cpb cells: 4N per cell (one per face point),
-// rounded up to whole warps
-__host__ __device__ constexpr int stage_threads(int n, int cpb) { return (4 * n * cpb + 31) / 32 * 32; }
+// threads per cell: one per face point (4N); the 6-cell tile gives each
+// solution point its own thread where there are more of those (N*N > 4N, N
+// >= 5), so that the residual phase takes one round (measured the fastest
+// tile of the mixed and exact forms at N = 5, with at most 80 registers)
+__host__ __device__ constexpr int stage_tpc(int n, int cpb) { return cpb == 6 && n * n > 4 * n ? n * n : 4 * n; }
+// threads of a CTA owning cpb cells, rounded up to whole warps
+__host__ __device__ constexpr int stage_threads(int n, int cpb) { return (stage_tpc(n, cpb) * cpb + 31) / 32 * 32; }
 
 // operators in kernel parameter space (row-major)
 struct Ops {
@@ -264,12 +268,12 @@ template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_byt
 
 // CTAs per SM the kernel is compiled for: as many as the 228 KB of shared
 // memory per SM hold (1 KB per CTA is the driver's), but no fewer than 96
-// registers per thread
+// registers per thread (80 for the 6-cell tile)
 template <int N, int CPB, typename R, bool DIAG> constexpr int stage_min_blocks()
 {
     int b = (int)((228 * 1024) / (stage_smem_bytes<N, CPB, R, DIAG>() + 1024));
     b = b < 1 ? 1 : (b > 8 ? 8 : b);
-    while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < 96) b--;
+    while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < (CPB == 6 ? 80 : 96)) b--;
     return b;
 }
 
@@ -973,13 +977,19 @@ template <int N, int CPB, typename R, bool DIAG, bool EXACT>
 __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
     stage_kernel(const StageArgs a, const Ops ops)
 {
-    if (a.tiles && a.persistent) {
-        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-            if (!stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, t)) return;
-            __syncthreads();  // tile t's last shared-memory reads before tile t+grid stages
-        }
-    } else {
-        stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, blockIdx.x);
+    stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, blockIdx.x);
+}
+
+// a batch's stage as a persistent launch: each CTA walks the tile table with
+// a grid stride (a kernel of its own, so that the one-tile kernel carries no
+// loop state)
+template <int N, int CPB, typename R, bool DIAG, bool EXACT>
+__global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
+    stage_kernel_persistent(const StageArgs a, const Ops ops)
+{
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        if (!stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, t)) return;
+        __syncthreads();  // tile t's last shared-memory reads before tile t+grid stages
     }
 }
 

@@ -60,7 +60,7 @@ def test_compresid_exact(name):
 
 
 @pytest.mark.parametrize("name", SMALL)
-@pytest.mark.parametrize("cpb", [4, 8, 16])
+@pytest.mark.parametrize("cpb", [4, 6, 8, 16])
 def test_rk_s5p3_exact(name, cpb):
     m, t, ph, Q, o, s = _pair(name, cpb=cpb)
     dt = 2e-3
@@ -99,9 +99,17 @@ def test_mixed_one_step(name):
     assert rel_l2(s.state()["Q"], o.state()["Q"]) <= 1e-6
 
 
+# mixed form after 500 steps of the 32 x 64 cylinder, against the oracle
+# (measured 1.4e-7 over all nine variables; per variable at most 1.1e-7 of
+# the state's norm)
+MIXED_500_ALL = 3e-7
+MIXED_500_STATE_SCALE = 2e-7
+
+
 def test_config1_500_steps():
     """Cylinder 32 x 64, p = 3, 500 RK3 steps at CFL 0.3 (Ms = 0.5, MA = 2):
-    exact form bit-exact, FP64 form <= 1e-9, mixed form reported."""
+    exact form bit-exact, FP64 form <= 1e-9, mixed form within the measured
+    bounds above, over all variables and per variable at the state's scale."""
     c = cases.cylinder_case(32, 64, 4, ms=0.5, ma=2.0)
     t = host.build_tables(c.mesh, c.N)
     Q0 = c.initial_state(t)
@@ -121,7 +129,10 @@ def test_config1_500_steps():
         s.close()
     assert np.array_equal(out["fp64_exact"], ref)
     assert rel_l2(out["fp64"], ref) <= 1e-9
-    assert rel_l2(out["mixed"], ref) <= 1e-4  # measured value is reported by bench.py
+    assert rel_l2(out["mixed"], ref) <= MIXED_500_ALL
+    scale = np.linalg.norm(ref)
+    per_var = [float(np.linalg.norm(out["mixed"][k] - ref[k]) / scale) for k in range(9)]
+    assert max(per_var) <= MIXED_500_STATE_SCALE, per_var
 
 
 def test_bad_tables_rejected():
