@@ -325,7 +325,10 @@ def run_ours(args):
         "accuracy": acc,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "bytes_per_dof_stage": bpd, "kernel": "stage_kernel<5,8,float> (mixed)",
+                     "traffic_note": "mean DRAM bytes per stage launch over the 5 stages of a step (ncu, "
+                                     "profiles/traffic.json); algorithmic bytes per launch: "
+                                     f"{dof * bpd:.4g}",
+                     "bytes_per_dof_stage": bpd, "kernel": f"stage_kernel<{c.N},{TILES['mixed']['cells_per_cta']},float> (mixed)",
                      "fp64_side": {"ref_ops_per_dof_stage": REF_OPS_PER_DOF_STAGE_N5,
                                    "ref_ops_per_byte": REF_OPS_PER_DOF_STAGE_N5 / bpd,
                                    "fp64_form_ref_ops_per_s": val["fp64"] * REF_OPS_PER_DOF_STAGE_N5,

@@ -150,45 +150,20 @@ SDDC_HD void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *Fnr, R n0, R n1, int
     }
     const R Vn_l = ul * unit_x + vl * unit_y, Bn_l = Bxl * unit_x + Byl * unit_y;
     const R Vn_r = ur * unit_x + vr * unit_y, Bn_r = Bxr * unit_x + Byr * unit_y;
-
-    Fnl[0] = Qfl[0] * Vn_l;
-    Fnl[1] = (Qfl[1] * Vn_l + pl * unit_x) - Bxl * Bn_l;
-    Fnl[2] = (Qfl[2] * Vn_l + pl * unit_y) - Byl * Bn_l;
-    Fnl[3] = Qfl[3] * Vn_l - Bzl * Bn_l;
-    Fnl[4] = ((Qfl[4] - (R)0.5 * (psil * psil)) + pl) * Vn_l - Bn_l * ((ul * Bxl + vl * Byl) + wl * Bzl);
-    Fnl[5] = (vl * Bxl - ul * Byl) * unit_y;
-    Fnl[6] = (ul * Byl - vl * Bxl) * unit_x;
-    Fnl[7] = Bzl * Vn_l - wl * Bn_l;
-    Fnr[0] = Qfr[0] * Vn_r;
-    Fnr[1] = (Qfr[1] * Vn_r + pr * unit_x) - Bxr * Bn_r;
-    Fnr[2] = (Qfr[2] * Vn_r + pr * unit_y) - Byr * Bn_r;
-    Fnr[3] = Qfr[3] * Vn_r - Bzr * Bn_r;
-    Fnr[4] = ((Qfr[4] - (R)0.5 * (psir * psir)) + pr) * Vn_r - Bn_r * ((ur * Bxr + vr * Byr) + wr * Bzr);
-    Fnr[5] = (vr * Bxr - ur * Byr) * unit_y;
-    Fnr[6] = (ur * Byr - vr * Bxr) * unit_x;
-    Fnr[7] = Bzr * Vn_r - wr * Bn_r;
-    // GLM terms
-    Fnl[4] = Fnl[4] + c_h * psil * Bn_l;
-    Fnr[4] = Fnr[4] + c_h * psir * Bn_r;
-    Fnl[5] = Fnl[5] + c_h * psil * unit_x;
-    Fnr[5] = Fnr[5] + c_h * psir * unit_x;
-    Fnl[6] = Fnl[6] + c_h * psil * unit_y;
-    Fnr[6] = Fnr[6] + c_h * psir * unit_y;
-    Fnl[8] = c_h * Bn_l;
-    Fnr[8] = c_h * Bn_r;
-    // fast magnetosonic speed of the averaged state
-    pl = pl - (R)0.5 * NORM_Bl;
-    pr = pr - (R)0.5 * NORM_Br;
+    // fast magnetosonic speed of the averaged state first, so that each
+    // flux component is formed and combined in turn (fewer values live at
+    // once); every component's arithmetic is the reference's
+    const R pgl = pl - (R)0.5 * NORM_Bl, pgr = pr - (R)0.5 * NORM_Br;
     const R Bx = (R)0.5 * (Bxl + Bxr), By = (R)0.5 * (Byl + Byr), Bz = (R)0.5 * (Bzl + Bzr);
     const R bn = Bx * unit_x + By * unit_y;
     R c_a, c_d, c_n;
     if constexpr (EX) {
-        c_a = (R)kGam * (pl + pr) / (Qfl[0] + Qfr[0]);
+        c_a = (R)kGam * (pgl + pgr) / (Qfl[0] + Qfr[0]);
         c_d = ((Bx * Bx + By * By) + Bz * Bz) / ((R)0.5 * (Qfl[0] + Qfr[0]));
         c_n = bn * bn / ((R)0.5 * (Qfl[0] + Qfr[0]));
     } else {
         const R rs = (R)1 / (Qfl[0] + Qfr[0]);
-        c_a = (R)kGam * (pl + pr) * rs;
+        c_a = (R)kGam * (pgl + pgr) * rs;
         c_d = (R)2 * ((Bx * Bx + By * By) + Bz * Bz) * rs;
         c_n = (R)2 * bn * bn * rs;
     }
@@ -198,13 +173,25 @@ SDDC_HD void rusanov(const R *Qfl, const R *Qfr, R *Fnl, R *Fnr, R n0, R n1, int
     const R eigv = (R)0.5 * Abs(Vn_l + Vn_r) + c_f;
     const R sl = magnorm * (R)sign_l;
     const R slr = (R)(sign_l * sign_r);
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        R f = (R)0.5 * ((Fnl[k] + Fnr[k]) - eigv * (Qfr[k] - Qfl[k]));
+    auto put = [&](int k, R fl, R fr) {
+        R f = (R)0.5 * ((fl + fr) - eigv * (Qfr[k] - Qfl[k]));
         f = sl * f;
         Fnl[k] = f;
         Fnr[k] = slr * f;
-    }
+    };
+    put(0, Qfl[0] * Vn_l, Qfr[0] * Vn_r);
+    put(1, (Qfl[1] * Vn_l + pl * unit_x) - Bxl * Bn_l, (Qfr[1] * Vn_r + pr * unit_x) - Bxr * Bn_r);
+    put(2, (Qfl[2] * Vn_l + pl * unit_y) - Byl * Bn_l, (Qfr[2] * Vn_r + pr * unit_y) - Byr * Bn_r);
+    put(3, Qfl[3] * Vn_l - Bzl * Bn_l, Qfr[3] * Vn_r - Bzr * Bn_r);
+    // with the GLM terms (getrusanov.f90:77-89)
+    put(4, (((Qfl[4] - (R)0.5 * (psil * psil)) + pl) * Vn_l - Bn_l * ((ul * Bxl + vl * Byl) + wl * Bzl)) +
+               c_h * psil * Bn_l,
+        (((Qfr[4] - (R)0.5 * (psir * psir)) + pr) * Vn_r - Bn_r * ((ur * Bxr + vr * Byr) + wr * Bzr)) +
+            c_h * psir * Bn_r);
+    put(5, (vl * Bxl - ul * Byl) * unit_y + c_h * psil * unit_x, (vr * Bxr - ur * Byr) * unit_y + c_h * psir * unit_x);
+    put(6, (ul * Byl - vl * Bxl) * unit_x + c_h * psil * unit_y, (ur * Byr - vr * Bxr) * unit_x + c_h * psir * unit_y);
+    put(7, Bzl * Vn_l - wl * Bn_l, Bzr * Vn_r - wr * Bn_r);
+    put(8, c_h * Bn_l, c_h * Bn_r);
     eigv_out = eigv;
     const R um = Max(Max((R)0.5 * Abs(ul + ur), (R)0.5 * Abs(vl + vr)), (R)0.5 * Abs(wl + wr));
     if (um > umax) umax = um;
