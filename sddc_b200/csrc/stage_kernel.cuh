@@ -591,14 +591,10 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
 
     // ---- C: B gradient, sources and the residual per solution point ------------
     // in a time step the RK coefficients of the stage (phase E runs here)
-    double cf[6];
-    if constexpr (!DIAG) {
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            const double dt = a.cases ? a.cases[cs].dt : a.dt;
-            cf[i] = ((a.dt_mask >> i) & 1u) ? a.cb[i] * dt : a.cb[i];
-        }
-    }
+    // formed where used, from the kernel parameters (not held in registers
+    // through the phase)
+    const double cdt = a.cases ? a.cases[cs].dt : a.dt;
+    auto cf = [&](int i) -> double { return ((a.dt_mask >> i) & 1u) ? a.cb[i] * cdt : a.cb[i]; };
     double part_r = 0.0, part_d = 0.0;
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
@@ -744,13 +740,13 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
                 const double qk = q[k], r = res[k];
                 double o;
                 switch (kind) {
-                case kRkAxpy: o = qk + cf[0] * r; break;
-                case kRkTwoReg: o = (cf[1] * ap[k] + cf[2] * qk) + cf[0] * r; break;
-                case kRkTwoRegT: o = (cf[1] * ap[k] + cf[2] * qk) + (cf[0] * r) * cf[3]; break;
+                case kRkAxpy: o = qk + cf(0) * r; break;
+                case kRkTwoReg: o = (cf(1) * ap[k] + cf(2) * qk) + cf(0) * r; break;
+                case kRkTwoRegT: o = (cf(1) * ap[k] + cf(2) * qk) + (cf(0) * r) * cf(3); break;
                 default:
-                    o = ((((cf[1] * a.reg_a[g + k] + cf[2] * a.reg_b[g + k]) + cf[3] * a.reg_c[g + k]) + cf[4] * qk) +
-                         cf[5] * a.reg_d[g + k]) +
-                        cf[0] * r;
+                    o = ((((cf(1) * a.reg_a[g + k] + cf(2) * a.reg_b[g + k]) + cf(3) * a.reg_c[g + k]) + cf(4) * qk) +
+                         cf(5) * a.reg_d[g + k]) +
+                        cf(0) * r;
                     break;
                 }
                 ap[k] = o;
@@ -953,8 +949,9 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
             atomic_max_nonneg(&maxima[2 * a.slot_w], m0);
             atomic_max_nonneg(&maxima[2 * a.slot_w + 1], m1);
             if (first_tile) {  // carry the previous stages' maxima forward
-                atomic_max_nonneg(&maxima[2 * a.slot_w], eig_r);
-                atomic_max_nonneg(&maxima[2 * a.slot_w + 1], um_r);
+                // (re-read: slot_r is not written during the stage)
+                atomic_max_nonneg(&maxima[2 * a.slot_w], maxima[2 * a.slot_r]);
+                atomic_max_nonneg(&maxima[2 * a.slot_w + 1], maxima[2 * a.slot_r + 1]);
             }
             if (a.mon_part) {
                 a.mon_part[2 * tile] = s0;
