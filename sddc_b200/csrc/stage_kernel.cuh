@@ -204,7 +204,13 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes
 template <int N, typename R, bool DIAG> struct Smem {
     static constexpr int NQ = 9 * N * N;
     static constexpr int NP = N + 1;
-    static constexpr int NG = DIAG ? 9 : 2;  // variables of the face-averaged state kept for gradients
+    static constexpr int NG = DIAG ? 9 : (sizeof(R) == 4 ? 1 : 2);  // variables of the face-averaged state kept
+    // normals staged in shared memory (the mixed form's time step reads them
+    // from global memory where used)
+    static constexpr bool kStageNrm = DIAG || sizeof(R) == 8;
+    // the mixed form's time step also keeps the block reductions at one slot
+    // per warp and no AV operators (6 CTAs per SM at the 6-cell tile, N = 5)
+    static constexpr bool kLean = !DIAG && sizeof(R) == 4;
     static constexpr int kF = 2 * N * NP * 9;   // R per cell: state then flux at every flux point
     static constexpr int kV = 2 * N * NP * NG;  // R per cell: face-averaged state at every flux point
     static constexpr int kLow = 2 * (N - 1) * (N - 1);
@@ -260,20 +266,21 @@ template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_byt
 {
     using S = Smem<N, R, DIAG>;
     // sQ, sA, sJac; the sensor's sJz and sLow in residual evaluations only
-    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) + 4 * 32 +
-               2 * (N - 1) * N;
-    size_t r = (size_t)CPB * (S::kF + S::kV + 2 * MetLayout<N>::kFam) + 2 * (N + 1) * N;
+    size_t d = (size_t)CPB * (2 * S::NQ + MetLayout<N>::kJacPad + (DIAG ? N * N + S::kLow : 0)) +
+               4 * (S::kLean ? stage_threads(N, CPB) / 32 : 32) + (S::kLean ? 0 : 2 * (N - 1) * N);
+    size_t r = (size_t)CPB * (S::kF + S::kV + (S::kStageNrm ? 2 * MetLayout<N>::kFam : 0)) + 2 * (N + 1) * N;
     return d * sizeof(double) + r * sizeof(R);
 }
 
 // CTAs per SM the kernel is compiled for: as many as the 228 KB of shared
 // memory per SM hold (1 KB per CTA is the driver's), but no fewer than 96
-// registers per thread (80 for the 6-cell tile)
+// registers per thread (64 for the 6-cell tile: 6 CTAs of 160 threads at
+// N = 5 in the mixed form, measured faster than 5 CTAs with 80 registers)
 template <int N, int CPB, typename R, bool DIAG> constexpr int stage_min_blocks()
 {
     int b = (int)((228 * 1024) / (stage_smem_bytes<N, CPB, R, DIAG>() + 1024));
     b = b < 1 ? 1 : (b > 8 ? 8 : b);
-    while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < (CPB == 6 ? 80 : 96)) b--;
+    while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < (CPB == 6 ? 64 : 96)) b--;
     return b;
 }
 
@@ -304,13 +311,14 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     double *sJac = sQ + CPB * NQ;                                // [CPB][NJ]
     double *sJz = sJac + CPB * NJ;                               // [CPB][NN]  Jz^2 for the sensor (DIAG)
     double *sLow = sJz + (DIAG ? CPB * NN : 0);                  // [CPB][kLow] (DIAG)
-    double *sRed = sLow + (DIAG ? CPB * S::kLow : 0);            // [4][32] block reductions
+    constexpr int NWR = S::kLean ? NT / 32 : 32;
+    double *sRed = sLow + (DIAG ? CPB * S::kLow : 0);            // [4][NWR] block reductions
     // residual (DIAG); in a time step the RK register, then the output
-    double *sA = sRed + 4 * 32;                                  // [CPB][NQ]
+    double *sA = sRed + 4 * NWR;                                 // [CPB][NQ]
     double *sOpH = sA + CPB * NQ;                                // [N-1][N]  AV projection
-    double *sOpHL = sOpH + (N - 1) * N;                          // [N][N-1]  AV prolongation
-    R *sNrm = reinterpret_cast<R *>(sOpHL + N * (N - 1));        // [CPB][NM] flux-point normals
-    R *sF = sNrm + CPB * NM;                                     // [CPB][2][N][NP][9]
+    double *sOpHL = sOpH + (S::kLean ? 0 : (N - 1) * N);         // [N][N-1]  AV prolongation (DIAG)
+    R *sNrm = reinterpret_cast<R *>(sOpHL + (S::kLean ? 0 : N * (N - 1)));  // [CPB][NM] flux-point normals
+    R *sF = sNrm + (S::kStageNrm ? CPB * NM : 0);                // [CPB][2][N][NP][9]
     R *sV = sF + CPB * S::kF;                                    // [CPB][2][N][NP][NG]
     // operators read with lane-dependent indices live in shared memory
     // (divergent reads of kernel parameters serialise per address)
@@ -364,10 +372,10 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         sAbort = 0;
         if (bulk) {
             mbar_init(&sBar, 1);
-            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + nbytes + jbytes + (want_ra ? qbytes : 0)));
+            mbar_expect_tx(&sBar, (unsigned)(qbytes + mbytes + (S::kStageNrm ? nbytes : 0) + jbytes + (want_ra ? qbytes : 0)));
             bulk_g2s(sQ, qsrc, (unsigned)qbytes, &sBar);
             if (split) {
-                bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
+                if (S::kStageNrm) bulk_g2s(sNrm, nsrc, (unsigned)nbytes, &sBar);
                 bulk_g2s(sJac, jsrc, (unsigned)jbytes, &sBar);
             } else {
                 bulk_g2s(sMetRaw, msrc0, (unsigned)mbytes, &sBar);
@@ -379,10 +387,11 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         sOpL[k] = opL<R>(ops, k);
         sOpM[k] = opM<R>(ops, k);
     }
-    for (int k = tid; k < (N - 1) * N; k += NT) {
-        sOpH[k] = ops.H[k];
-        sOpHL[k] = ops.HL[k];
-    }
+    if constexpr (!S::kLean)
+        for (int k = tid; k < (N - 1) * N; k += NT) {
+            sOpH[k] = ops.H[k];
+            sOpHL[k] = ops.HL[k];
+        }
     if (!bulk) {
         // batches of kU independent loads per thread before their stores, so
         // that each thread keeps several loads in flight
@@ -399,7 +408,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         };
         stage_copy(sQ, qsrc, ncl * NQ);
         if (split) {
-            stage_copy(sNrm, nsrc, ncl * NM);
+            if (S::kStageNrm) stage_copy(sNrm, nsrc, ncl * NM);
             stage_copy(sJac, jsrc, ncl * NJ);
         } else {
             stage_copy(sMetRaw, msrc0, ncl * ML::kSize);
@@ -423,7 +432,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         for (int k = tid; k < ncl * ML::kSize; k += NT) {
             const int c = k / ML::kSize, o = k - c * ML::kSize;
             const double v = sMetRaw[k];
-            if (o < NM) sNrm[c * NM + o] = (R)v;
+            if (o < NM) { if (S::kStageNrm) sNrm[c * NM + o] = (R)v; }
             else if (o < NM + NN) sJac[c * NJ + (o - NM)] = v;
         }
         __syncthreads();
@@ -460,8 +469,17 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         for (int k = 0; k < 9; k++) q[k] = slot[k];
         if (!(q[0] > (R)0)) err |= kErrNonPositiveDensity;
         iflux<R, EX>(q, c_h, umax, F, G);
-        const R *nrm = sNrm + c * NM + ML::normal(f, l, r);
-        const R n0 = nrm[0], n1 = nrm[1];
+        R n0, n1;
+        if constexpr (S::kStageNrm) {
+            const R *nrm = sNrm + c * NM + ML::normal(f, l, r);
+            n0 = nrm[0]; n1 = nrm[1];
+        } else if (split) {
+            const R *gn = reinterpret_cast<const R *>(a.nrm) + (size_t)(c0 + c) * NM + ML::normal(f, l, r);
+            n0 = __ldg(gn); n1 = __ldg(gn + 1);
+        } else {
+            const double *gn = a.met + (size_t)(c0 + c) * ML::kSize + ML::normal(f, l, r);
+            n0 = (R)__ldg(gn); n1 = (R)__ldg(gn + 1);
+        }
 #pragma unroll
         for (int k = 0; k < 9; k++) slot[k] = F[k] * n0 + G[k] * n1;
         R *vs = sV + c * S::kV + ((f * N + l) * NP + r) * NG;
@@ -489,7 +507,17 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         for (int k = 0; k < 9; k++) own[k] = slot[k];
         const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
         const int kind = rec.y & 0xff;
-        const R *onrm = sNrm + c * NM + ML::normal(fam, line, r);
+        R on0, on1;
+        if constexpr (S::kStageNrm) {
+            const R *nrm = sNrm + c * NM + ML::normal(fam, line, r);
+            on0 = nrm[0]; on1 = nrm[1];
+        } else if (split) {
+            const R *gn = reinterpret_cast<const R *>(a.nrm) + (size_t)(c0 + c) * NM + ML::normal(fam, line, r);
+            on0 = __ldg(gn); on1 = __ldg(gn + 1);
+        } else {
+            const double *gn = a.met + (size_t)(c0 + c) * ML::kSize + ML::normal(fam, line, r);
+            on0 = (R)__ldg(gn); on1 = (R)__ldg(gn + 1);
+        }
         R n0, n1;
         int sign_l, sign_r;
         const bool pair = kind == kFaceLeft || kind == kFaceRight;
@@ -501,7 +529,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
             const R *rv = reinterpret_cast<const R *>(a.proc_recv) + ((size_t)rec.x * N + (N - nfp)) * 9;
 #pragma unroll
             for (int k = 0; k < 9; k++) other[k] = rv[k];
-            n0 = onrm[0]; n1 = onrm[1];
+            n0 = on0; n1 = on1;
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
         } else if (pair) {
@@ -514,7 +542,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
 #pragma unroll
             for (int k = 0; k < 9; k++) other[k] = tp[trace_at<N>(pc, plf, N - nfp, k)];
             if (!own_right) {
-                n0 = onrm[0]; n1 = onrm[1];
+                n0 = on0; n1 = on1;
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = pr == N ? -1 : 1;
             } else {
@@ -533,7 +561,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
                 sign_r = r == N ? -1 : 1;
             }
         } else {
-            n0 = onrm[0]; n1 = onrm[1];
+            n0 = on0; n1 = on1;
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
             bc_ghost<R, EX>(kind, own, n0, n1, a.vismode, a.cases ? a.cases[cs].fs : a.fs, other);
@@ -560,7 +588,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         } else {
             const R bxa = (R)0.5 * Ql[5] + (R)0.5 * Qr[5], bya = (R)0.5 * Ql[6] + (R)0.5 * Qr[6];
             if constexpr (kBn) {
-                vs[0] = bxa * onrm[0] + bya * onrm[1];  // this cell's normal
+                vs[0] = bxa * on0 + bya * on1;  // this cell's normal
             } else {
                 vs[0] = bxa;
                 vs[1] = bya;
@@ -599,7 +627,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     for (int t = tid; t < ncl * NN; t += NT) {
         const int i = t % N, j = (t / N) % N, c = t / NN;
         const int cell = c0 + c;
-        const R *met = sNrm + c * NM;
+        const R *met = S::kStageNrm ? sNrm + c * NM : nullptr;  // used only where the normals are staged
         // Jac, or its reciprocal when the split array holds reciprocals (the
         // exact form divides by Jac, as the reference does; the others multiply
         // by 1/Jac, rounded once, on the host or here)
@@ -932,9 +960,9 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         }
         if (lane == 0) {
             sRed[wid] = em;
-            sRed[32 + wid] = um;
-            sRed[64 + wid] = pr;
-            sRed[96 + wid] = pd;
+            sRed[NWR + wid] = um;
+            sRed[2 * NWR + wid] = pr;
+            sRed[3 * NWR + wid] = pd;
             if (e) atomicOr(a.err_flags, e);
         }
         __syncthreads();
@@ -942,9 +970,9 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
             double m0 = 0.0, m1 = 0.0, s0 = 0.0, s1 = 0.0;
             for (int w = 0; w < NW; w++) {
                 m0 = sRed[w] > m0 ? sRed[w] : m0;
-                m1 = sRed[32 + w] > m1 ? sRed[32 + w] : m1;
-                s0 += sRed[64 + w];
-                s1 += sRed[96 + w];
+                m1 = sRed[NWR + w] > m1 ? sRed[NWR + w] : m1;
+                s0 += sRed[2 * NWR + w];
+                s1 += sRed[3 * NWR + w];
             }
             atomic_max_nonneg(&maxima[2 * a.slot_w], m0);
             atomic_max_nonneg(&maxima[2 * a.slot_w + 1], m1);
