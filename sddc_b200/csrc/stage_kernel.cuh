@@ -1009,17 +1009,13 @@ __device__ __forceinline__ void stage_tiles_persistent(const StageArgs &a, const
     }
 }
 
-// The persistent walk lives in the one kernel when kPersistInline (the mixed
-// form: with the 80-register cap of its 6-cell tile that build ran 7% faster,
-// same-box timing) and in a kernel of its own otherwise (the FP64 forms: the
-// one-tile kernel then carries no loop state, 2% faster at their tiles).
+// One CTA per tile.  The persistent walk is a kernel of its own, so that the
+// one-tile kernel carries no loop state.
 template <int N, int CPB, typename R, bool DIAG, bool EXACT>
 __global__ void __launch_bounds__(stage_threads(N, CPB), (stage_min_blocks<N, CPB, R, DIAG>()))
     stage_kernel(const StageArgs a, const Ops ops)
 {
-    constexpr bool kPersistInline = sizeof(R) != sizeof(double);
-    if (kPersistInline && a.tiles && a.persistent) stage_tiles_persistent<N, CPB, R, DIAG, EXACT>(a, ops);
-    else stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, blockIdx.x);
+    stage_tile<N, CPB, R, DIAG, EXACT>(a, ops, blockIdx.x);
 }
 
 template <int N, int CPB, typename R, bool DIAG, bool EXACT>

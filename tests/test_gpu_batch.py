@@ -26,7 +26,7 @@ def _large_members():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "mixed"])
-@pytest.mark.parametrize("cpb", [4, 8])
+@pytest.mark.parametrize("cpb", [4, 6, 8])
 @pytest.mark.parametrize("persistent", [False, True])
 def test_batch_equals_separate_runs(precision, cpb, persistent):
     members = _members() if not persistent else _large_members()
