@@ -405,8 +405,12 @@ def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200, max_steps=0, forms=("fp
     dof = c.mesh.ncell * c.N * c.N
     out, res = {}, {"workload": f"Orszag-Tang {n}x{n} periodic, p=3 (N=4), RK_S5P3, CFL 0.3, t_end={t_end}",
                     "dof": dof, "dt": dt, "steps": nsteps}
+    from sddc_b200 import autotune
+
     for prec in forms:
-        s = Solver(t, c.physics, precision=prec)
+        cpb, _ = autotune.tune(t, c.physics, Q0, dt, prec, steps=2)
+        res.setdefault("cells_per_cta", {})[prec] = cpb
+        s = Solver(t, c.physics, precision=prec, cells_per_cta=cpb)
         s.set_state(Q0)
         m0 = s.monitor()["mass"]
         st = torch.cuda.ExternalStream(s.stream_handle())
