@@ -9,7 +9,9 @@
 // Work split: one CTA owns CPB consecutive cells and stages them in shared
 // memory.  Phases, separated by __syncthreads:
 //   A  Lagrange interpolation of every line of solution points to its N+1
-//      flux points (one thread per cell x family x line x variable);
+//      flux points (one thread per cell x line index x variable: the xi-
+//      and eta-line of one index share the operator row, so their sums go
+//      through paired FMAs, FFMA2 in the mixed form);
 //   B1 physical flux at the interior flux points (thread per point);
 //   B2 Rusanov flux at the 4N face points of each cell (thread per point).
 //      The neighbour's trace at the face point comes from the trace buffer
@@ -223,6 +225,30 @@ template <> __device__ __forceinline__ float opL<float>(const Ops &o, int i) { r
 template <typename R> __device__ __forceinline__ R opM(const Ops &o, int i);
 template <> __device__ __forceinline__ double opM<double>(const Ops &o, int i) { return o.M[i]; }
 template <> __device__ __forceinline__ float opM<float>(const Ops &o, int i) { return o.Mf[i]; }
+
+
+// two lanes of the arithmetic type through one paired FMA (FFMA2 for float,
+// each component rounded as fmaf; for double two scalar multiply-adds, in
+// the order a + x*y of the scalar code)
+template <typename R> struct Pair2;
+template <> struct Pair2<float> { using T = float2; };
+template <> struct Pair2<double> { using T = double2; };
+template <typename R> using P2 = typename Pair2<R>::T;
+__device__ __forceinline__ float2 fma2(float2 x, float2 y, float2 z) { return __ffma2_rn(x, y, z); }
+__device__ __forceinline__ double2 fma2(double2 x, double2 y, double2 z)
+{
+    return make_double2(z.x + x.x * y.x, z.y + x.y * y.y);
+}
+template <typename R> __device__ __forceinline__ P2<R> splat2(R v)
+{
+    P2<R> p;
+    p.x = v;
+    p.y = v;
+    return p;
+}
+
+template <typename R> __device__ __forceinline__ P2<R> opL2(const Ops &o, int i) { return splat2<R>(opL<R>(o, i)); }
+template <typename R> __device__ __forceinline__ P2<R> opM2(const Ops &o, int i) { return splat2<R>(opM<R>(o, i)); }
 
 // local face lf (1..4), face point nfp (1..N) -> flux point (family, line, point)
 // (face2fpconnec, initsetup.f90:347-383)
@@ -439,19 +465,26 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     }
 
     // ---- A: interpolate every line to its flux points ---------------------------
-    for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
-        const int v = t % 9, l = (t / 9) % N, f = (t / (9 * N)) % 2, c = t / (18 * N);
-        const double *q = sQ + c * NQ;
-        R qs[N];
+    // one thread per (cell, line index l, variable): xi-line l and eta-line l
+    // together, their sums paired (both use the same operator row)
+    for (int t = tid; t < ncl * N * 9; t += NT) {
+        const int v = t % 9, l = (t / 9) % N, c = t / (9 * N);
+        const double *q = sQ + c * NQ + v;
+        P2<R> qs[N];
 #pragma unroll
-        for (int s = 0; s < N; s++) qs[s] = (R)(f == 0 ? q[v + 9 * (s + N * l)] : q[v + 9 * (l + N * s)]);
-        R *out = sF + c * S::kF + (f * N + l) * NP * 9 + v;
+        for (int s = 0; s < N; s++) {
+            qs[s].x = (R)q[9 * (s + N * l)];
+            qs[s].y = (R)q[9 * (l + N * s)];
+        }
+        R *ox = sF + c * S::kF + l * NP * 9 + v;  // xi-line l (family 0)
+        R *oy = ox + N * NP * 9;                   // eta-line l (family 1)
 #pragma unroll
         for (int r = 0; r < NP; r++) {
-            R acc = (R)0;
+            P2<R> acc = splat2<R>((R)0);
 #pragma unroll
-            for (int s = 0; s < N; s++) acc = acc + qs[s] * opL<R>(ops, r * N + s);
-            out[r * 9] = acc;
+            for (int s = 0; s < N; s++) acc = fma2(qs[s], opL2<R>(ops, r * N + s), acc);
+            ox[r * 9] = acc.x;
+            oy[r * 9] = acc.y;
         }
     }
     __syncthreads();
@@ -598,21 +631,27 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     __syncthreads();
 
     // ---- C1: flux derivative along every line, in place ------------------------
-    // one thread per (cell, family, line, variable): the N+1 flux values of
-    // the line, d(i) = sum over r of F(r) * M(r, i) in the reference's order
-    // (compresid.f90:14-32), written over point slots 0..N-1 of the line
-    for (int t = tid; t < ncl * 2 * N * 9; t += NT) {
-        const int k = t % 9, l = (t / 9) % N, f = (t / (9 * N)) % 2, c = t / (18 * N);
-        R *col = sF + c * S::kF + (f * N + l) * NP * 9 + k;
-        R fv[NP];
+    // one thread per (cell, line index, variable), the xi- and eta-line of
+    // the index paired: the N+1 flux values of each line, d(i) = sum over r
+    // of F(r) * M(r, i) in the reference's order (compresid.f90:14-32),
+    // written over point slots 0..N-1 of the line
+    for (int t = tid; t < ncl * N * 9; t += NT) {
+        const int k = t % 9, l = (t / 9) % N, c = t / (9 * N);
+        R *cx = sF + c * S::kF + l * NP * 9 + k;  // xi-line l
+        R *cy = cx + N * NP * 9;                   // eta-line l
+        P2<R> fv[NP];
 #pragma unroll
-        for (int r = 0; r < NP; r++) fv[r] = col[r * 9];
+        for (int r = 0; r < NP; r++) {
+            fv[r].x = cx[r * 9];
+            fv[r].y = cy[r * 9];
+        }
 #pragma unroll
         for (int i = 0; i < N; i++) {
-            R d = (R)0;
+            P2<R> d = splat2<R>((R)0);
 #pragma unroll
-            for (int r = 0; r < NP; r++) d = d + fv[r] * opM<R>(ops, r * N + i);
-            col[i * 9] = d;
+            for (int r = 0; r < NP; r++) d = fma2(fv[r], opM2<R>(ops, r * N + i), d);
+            cx[i * 9] = d.x;
+            cy[i * 9] = d.y;
         }
     }
     __syncthreads();
@@ -936,12 +975,24 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
                 face_point<N>(lf, nfp, fam, line, r);
                 const R *q = qo + c * (PS * NN) + (fam == 0 ? PS * N * line : PS * line);
                 const int stride = fam == 0 ? PS : PS * N;
+                // variables in pairs (8-byte loads of the float copy, paired FMAs)
+                P2<R> Ls[N];
 #pragma unroll
-                for (int k = 0; k < 9; k++) {
+                for (int s = 0; s < N; s++) Ls[s] = splat2<R>(sOpL[r * N + s]);
+#pragma unroll
+                for (int k = 0; k < 8; k += 2) {
+                    P2<R> acc = splat2<R>((R)0);
+#pragma unroll
+                    for (int s = 0; s < N; s++)
+                        acc = fma2(*reinterpret_cast<const P2<R> *>(q + k + stride * s), Ls[s], acc);
+                    to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc.x;
+                    to[trace_at<N>(c0 + c, lf, nfp - 1, k + 1)] = acc.y;
+                }
+                {
                     R acc = (R)0;
 #pragma unroll
-                    for (int s = 0; s < N; s++) acc = acc + q[k + stride * s] * sOpL[r * N + s];
-                    to[trace_at<N>(c0 + c, lf, nfp - 1, k)] = acc;
+                    for (int s = 0; s < N; s++) acc = acc + q[8 + stride * s] * Ls[s].x;
+                    to[trace_at<N>(c0 + c, lf, nfp - 1, 8)] = acc;
                 }
             }
         }
