@@ -18,7 +18,9 @@
 //      (trace_at) that the stage producing the input published.  Each
 //      shared face is evaluated by both of its cells, each with the
 //      reference's left/right assignment, so both get the value the
-//      reference scatters to them;
+//      reference scatters to them.  Its loads from global memory are issued
+//      early: the face record before the staging wait, the neighbour's
+//      trace and the normals before B1 (after it in the exact form);
 //   C  divergence of the flux, gradient of (Bx, By) from the face-averaged
 //      flux-point states, Powell and GLM sources (thread per solution point);
 //   D  the AV smoothness sensor per cell (residual evaluations only);
@@ -368,6 +370,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     }
     // per-case data is read where it is used (kept out of registers)
     double *maxima = a.maxima + 10 * cs;
+    // the face record of this thread's face point (a cell has 4N face points
+    // and at least 4N threads: one face point per thread at most), loaded
+    // before the staging wait
+    static_assert(stage_tpc(N, CPB) >= 4 * N, "one face point per thread at most");
+    const bool has_fp = tid < ncl * 4 * N;
+    const int2 frec = has_fp ? __ldg(a.faces + (size_t)c0 * 4 + tid / N) : make_int2(0, 0);
 
     // ---- stage the state, the metrics and the operators ------------------------
     // The tile's state slice goes to sQ, its normals to sNrm and Jac to sJac
@@ -492,6 +500,62 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     R eigmax = (R)0, umax = (R)0;
     unsigned err = 0;
 
+    // ---- B2's inputs from global memory (the neighbour's trace or the
+    // received remote trace, the normals).  The forms other than the exact
+    // one gather them before B1, so that their latency overlaps the interior
+    // fluxes (measured faster there; slower in the exact form, which gathers
+    // them after B1)
+    constexpr bool kGatherEarly = !EX;
+    R other[9];
+    R on0 = (R)0, on1 = (R)0, pn0 = (R)0, pn1 = (R)0;
+    auto gather = [&]() {
+        if (has_fp) {
+            const int nfp = 1 + tid % N, lf = 1 + (tid / N) % 4, c = tid / (4 * N);
+            int fam, line, r;
+            face_point<N>(lf, nfp, fam, line, r);
+            const int kind = frec.y & 0xff;
+            if constexpr (S::kStageNrm) {
+                const R *nrm = sNrm + c * NM + ML::normal(fam, line, r);
+                on0 = nrm[0]; on1 = nrm[1];
+            } else if (split) {
+                const R *gn = reinterpret_cast<const R *>(a.nrm) + (size_t)(c0 + c) * NM + ML::normal(fam, line, r);
+                on0 = __ldg(gn); on1 = __ldg(gn + 1);
+            } else {
+                const double *gn = a.met + (size_t)(c0 + c) * ML::kSize + ML::normal(fam, line, r);
+                on0 = (R)__ldg(gn); on1 = (R)__ldg(gn + 1);
+            }
+            if (kind == kFaceProc) {
+                // the received trace, remote point N+1-nfp (procintflux_all.f90:83-99)
+                const R *rv = reinterpret_cast<const R *>(a.proc_recv) + ((size_t)frec.x * N + (N - nfp)) * 9;
+#pragma unroll
+                for (int k = 0; k < 9; k++) other[k] = rv[k];
+            } else if (kind == kFaceLeft || kind == kFaceRight) {
+                // partner point N-nfp+1 on the partner's local face; its trace was
+                // published by the stage that produced q_in
+                const int pc = frec.x, plf = (frec.y >> 8) & 0xff;
+                const R *tp = reinterpret_cast<const R *>(a.t_in);
+#pragma unroll
+                for (int k = 0; k < 9; k++) other[k] = tp[trace_at<N>(pc, plf, N - nfp, k)];
+                if (kind == kFaceRight) {
+                    // the left (partner) cell's normal, from the split array or
+                    // the packed record
+                    int pfam, pline, pr;
+                    face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
+                    if (split) {
+                        const R *pn = reinterpret_cast<const R *>(a.nrm) + (size_t)pc * NM + ML::normal(pfam, pline, pr);
+                        pn0 = __ldg(pn);
+                        pn1 = __ldg(pn + 1);
+                    } else {
+                        const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
+                        pn0 = (R)__ldg(pn);
+                        pn1 = (R)__ldg(pn + 1);
+                    }
+                }
+            }
+        }
+    };
+    if constexpr (kGatherEarly) gather();
+
     // ---- B1: interior flux points (inviscid_flux_interior) ---------------------
     for (int t = tid; t < ncl * 2 * N * (N - 1); t += NT) {
         const int r = 1 + t % (N - 1), l = (t / (N - 1)) % N, f = (t / ((N - 1) * N)) % 2,
@@ -529,67 +593,37 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
         }
     }
 
+    if constexpr (!kGatherEarly) gather();
+
     // ---- B2: face points (interfaceflux, CYCLOCFLUX, BCFLUX) -------------------
-    for (int t = tid; t < ncl * 4 * N; t += NT) {
-        const int nfp = 1 + t % N, lf = 1 + (t / N) % 4, c = t / (4 * N);
+    if (has_fp) {
+        const int nfp = 1 + tid % N, lf = 1 + (tid / N) % 4, c = tid / (4 * N);
         int fam, line, r;
         face_point<N>(lf, nfp, fam, line, r);
         R *slot = sF + c * S::kF + ((fam * N + line) * NP + r) * 9;
-        R own[9], other[9], Fl[9], Fr[9];
+        R own[9], Fl[9], Fr[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) own[k] = slot[k];
-        const int2 rec = a.faces[(size_t)(c0 + c) * 4 + (lf - 1)];
-        const int kind = rec.y & 0xff;
-        R on0, on1;
-        if constexpr (S::kStageNrm) {
-            const R *nrm = sNrm + c * NM + ML::normal(fam, line, r);
-            on0 = nrm[0]; on1 = nrm[1];
-        } else if (split) {
-            const R *gn = reinterpret_cast<const R *>(a.nrm) + (size_t)(c0 + c) * NM + ML::normal(fam, line, r);
-            on0 = __ldg(gn); on1 = __ldg(gn + 1);
-        } else {
-            const double *gn = a.met + (size_t)(c0 + c) * ML::kSize + ML::normal(fam, line, r);
-            on0 = (R)__ldg(gn); on1 = (R)__ldg(gn + 1);
-        }
+        const int kind = frec.y & 0xff;
         R n0, n1;
         int sign_l, sign_r;
         const bool pair = kind == kFaceLeft || kind == kFaceRight;
         const bool own_right = kind == kFaceRight;
         if (kind == kFaceProc) {
             // PROCINTFLUX / CYCREMFLUX (procintflux_all.f90:104-151): this
-            // cell is the left cell, with its own normal and sign_r = 1; the
-            // right state is the received trace, remote point N+1-nfp
-            const R *rv = reinterpret_cast<const R *>(a.proc_recv) + ((size_t)rec.x * N + (N - nfp)) * 9;
-#pragma unroll
-            for (int k = 0; k < 9; k++) other[k] = rv[k];
+            // cell is the left cell, with its own normal and sign_r = 1
             n0 = on0; n1 = on1;
             sign_l = r == 0 ? -1 : 1;
             sign_r = 1;
         } else if (pair) {
-            // partner point N-nfp+1 on the partner's local face; its trace was
-            // published by the stage that produced q_in
-            const int pc = rec.x, plf = (rec.y >> 8) & 0xff;
             int pfam, pline, pr;
-            face_point<N>(plf, N - nfp + 1, pfam, pline, pr);
-            const R *tp = reinterpret_cast<const R *>(a.t_in);
-#pragma unroll
-            for (int k = 0; k < 9; k++) other[k] = tp[trace_at<N>(pc, plf, N - nfp, k)];
+            face_point<N>((frec.y >> 8) & 0xff, N - nfp + 1, pfam, pline, pr);
             if (!own_right) {
                 n0 = on0; n1 = on1;
                 sign_l = r == 0 ? -1 : 1;
                 sign_r = pr == N ? -1 : 1;
             } else {
-                // the left (partner) cell's normal, from the split array or
-                // the packed record
-                if (split) {
-                    const R *pn = reinterpret_cast<const R *>(a.nrm) + (size_t)pc * NM + ML::normal(pfam, pline, pr);
-                    n0 = __ldg(pn);
-                    n1 = __ldg(pn + 1);
-                } else {
-                    const double *pn = a.met + (size_t)pc * ML::kSize + ML::normal(pfam, pline, pr);
-                    n0 = (R)__ldg(pn);
-                    n1 = (R)__ldg(pn + 1);
-                }
+                n0 = pn0; n1 = pn1;
                 sign_l = pr == 0 ? -1 : 1;
                 sign_r = r == N ? -1 : 1;
             }
