@@ -19,8 +19,9 @@
 //      shared face is evaluated by both of its cells, each with the
 //      reference's left/right assignment, so both get the value the
 //      reference scatters to them.  Its loads from global memory are issued
-//      early: the face record before the staging wait, the neighbour's
-//      trace and the normals before B1 (after it in the exact form);
+//      early in the FP64 and mixed forms: the face record before the
+//      staging wait, the neighbour's trace and the normals before B1 (all
+//      after B1 in the exact form);
 //   C  divergence of the flux, gradient of (Bx, By) from the face-averaged
 //      flux-point states, Powell and GLM sources (thread per solution point);
 //   D  the AV smoothness sensor per cell (residual evaluations only);
@@ -372,10 +373,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     double *maxima = a.maxima + 10 * cs;
     // the face record of this thread's face point (a cell has 4N face points
     // and at least 4N threads: one face point per thread at most), loaded
-    // before the staging wait
+    // before the staging wait (in the exact form with the rest of the face
+    // point's inputs, after B1: measured faster there)
     static_assert(stage_tpc(N, CPB) >= 4 * N, "one face point per thread at most");
     const bool has_fp = tid < ncl * 4 * N;
-    const int2 frec = has_fp ? __ldg(a.faces + (size_t)c0 * 4 + tid / N) : make_int2(0, 0);
+    int2 frec = make_int2(0, 0);
+    if (!EX && has_fp) frec = __ldg(a.faces + (size_t)c0 * 4 + tid / N);
 
     // ---- stage the state, the metrics and the operators ------------------------
     // The tile's state slice goes to sQ, its normals to sNrm and Jac to sJac
@@ -510,6 +513,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     R on0 = (R)0, on1 = (R)0, pn0 = (R)0, pn1 = (R)0;
     auto gather = [&]() {
         if (has_fp) {
+            if constexpr (EX) frec = __ldg(a.faces + (size_t)c0 * 4 + tid / N);
             const int nfp = 1 + tid % N, lf = 1 + (tid / N) % 4, c = tid / (4 * N);
             int fam, line, r;
             face_point<N>(lf, nfp, fam, line, r);
