@@ -112,6 +112,37 @@ SDDC_HD void iflux(const R *Q, R c_h, R &umax, R *F, R *G)
     }
 }
 
+// F n0 + G n1 at one flux point, formed directly along (n0, n1) (the FP64
+// and mixed forms; the exact form projects iflux's F and G as the reference
+// does): the same flux, associated differently; updates the running max of
+// |u|,|v|,|w|
+template <typename R>
+SDDC_HD void iflux_n(const R *Q, R c_h, R n0, R n1, R &umax, R *Fn)
+{
+    const R rho = Q[0], rhou = Q[1], rhov = Q[2], rhow = Q[3], rhoE = Q[4];
+    const R Bx = Q[5], By = Q[6], Bz = Q[7], psi = Q[8];
+    const R ri = (R)1 / rho;
+    const R u = rhou * ri, v = rhov * ri, w = rhow * ri;
+    const R pr = pressure_fast<R>(Q, ri);
+    const R NORM_B = Bx * Bx + By * By + Bz * Bz;
+    const R un = u * n0 + v * n1, bn = Bx * n0 + By * n1;
+    const R pt = pr + (R)0.5 * NORM_B;
+    const R ub = u * Bx + v * By + w * Bz;
+    const R eb = rhoE - (R)0.5 * psi * psi + pt;
+    const R cp = c_h * psi;
+    Fn[0] = rhou * n0 + rhov * n1;
+    Fn[1] = rhou * un + pt * n0 - Bx * bn;
+    Fn[2] = rhov * un + pt * n1 - By * bn;
+    Fn[3] = rhow * un - Bz * bn;
+    Fn[4] = un * eb - (ub - cp) * bn;
+    Fn[5] = Bx * un - u * bn + cp * n0;
+    Fn[6] = By * un - v * bn + cp * n1;
+    Fn[7] = Bz * un - w * bn;
+    Fn[8] = c_h * bn;
+    const R um = Max(Max(Abs(u), Abs(v)), Abs(w));
+    if (um > umax) umax = um;
+}
+
 // getrusanovflux, getrusanov.f90:1-125.  Returns the left cell's
 // computational flux in Fnl, the right cell's in Fnr and the wave speed in
 // eigv; updates the running max of the face-averaged velocity.

@@ -12,7 +12,8 @@
 //      flux points (one thread per cell x line index x variable: the xi-
 //      and eta-line of one index share the operator row, so their sums go
 //      through paired FMAs, FFMA2 in the mixed form);
-//   B1 physical flux at the interior flux points (thread per point);
+//   B1 physical flux at the interior flux points (thread per point; the
+//      FP64 and mixed forms form F n0 + G n1 directly along the normal);
 //   B2 Rusanov flux at the 4N face points of each cell (thread per point).
 //      The neighbour's trace at the face point comes from the trace buffer
 //      (trace_at) that the stage producing the input published.  Each
@@ -561,16 +562,8 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     if constexpr (kGatherEarly) gather();
 
     // ---- B1: interior flux points (inviscid_flux_interior) ---------------------
-    for (int t = tid; t < ncl * 2 * N * (N - 1); t += NT) {
-        const int r = 1 + t % (N - 1), l = (t / (N - 1)) % N, f = (t / ((N - 1) * N)) % 2,
-                  c = t / (2 * N * (N - 1));
-        R *slot = sF + c * S::kF + ((f * N + l) * NP + r) * 9;
-        R q[9], F[9], G[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) q[k] = slot[k];
-        if (!(q[0] > (R)0)) err |= kErrNonPositiveDensity;
-        iflux<R, EX>(q, c_h, umax, F, G);
-        R n0, n1;
+    // the normal of family f, line l, flux point r of cell c
+    auto normal_at = [&](int c, int f, int l, int r, R &n0, R &n1) {
         if constexpr (S::kStageNrm) {
             const R *nrm = sNrm + c * NM + ML::normal(f, l, r);
             n0 = nrm[0]; n1 = nrm[1];
@@ -581,8 +574,29 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
             const double *gn = a.met + (size_t)(c0 + c) * ML::kSize + ML::normal(f, l, r);
             n0 = (R)__ldg(gn); n1 = (R)__ldg(gn + 1);
         }
+    };
+    for (int t = tid; t < ncl * 2 * N * (N - 1); t += NT) {
+        const int r = 1 + t % (N - 1), l = (t / (N - 1)) % N, f = (t / ((N - 1) * N)) % 2,
+                  c = t / (2 * N * (N - 1));
+        R *slot = sF + c * S::kF + ((f * N + l) * NP + r) * 9;
+        R q[9];
 #pragma unroll
-        for (int k = 0; k < 9; k++) slot[k] = F[k] * n0 + G[k] * n1;
+        for (int k = 0; k < 9; k++) q[k] = slot[k];
+        if (!(q[0] > (R)0)) err |= kErrNonPositiveDensity;
+        R n0, n1;
+        normal_at(c, f, l, r, n0, n1);
+        if constexpr (EX) {
+            // the reference's F and G, projected
+            R F[9], G[9];
+            iflux<R, EX>(q, c_h, umax, F, G);
+#pragma unroll
+            for (int k = 0; k < 9; k++) slot[k] = F[k] * n0 + G[k] * n1;
+        } else {
+            R Fn[9];
+            iflux_n<R>(q, c_h, n0, n1, umax, Fn);
+#pragma unroll
+            for (int k = 0; k < 9; k++) slot[k] = Fn[k];
+        }
         R *vs = sV + c * S::kV + ((f * N + l) * NP + r) * NG;
         if constexpr (DIAG) {
 #pragma unroll
@@ -972,8 +986,9 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     }
 
     // ---- F: face traces of the output state for the next stage's neighbours ---
+    // (the barrier after phase C orders its output before these reads: in a
+    // time step nothing between them writes shared memory)
     if (!DIAG && a.t_out) {
-        __syncthreads();
         R *to = reinterpret_cast<R *>(a.t_out);
         // the output state: sA (double), or its float copy over the state
         // slots (9 floats at the start of each point's 9 doubles)
@@ -1040,7 +1055,16 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const Ops &ops, c
     {
         const int lane = tid & 31, wid = tid >> 5;
         constexpr int NW = (NT + 31) / 32;
-        double em = warp_max((double)eigmax), um = warp_max((double)umax);
+        double em, um;
+        if constexpr (sizeof(R) == sizeof(float)) {
+            // the maxima are non-negative (never raised by NaN), and
+            // non-negative floats order as their bit patterns
+            em = (double)__uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(eigmax)));
+            um = (double)__uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(umax)));
+        } else {
+            em = warp_max((double)eigmax);
+            um = warp_max((double)umax);
+        }
         unsigned e = __reduce_or_sync(0xffffffffu, err);
         double pr = 0.0, pd = 0.0;
         if (a.mon_part) {
