@@ -328,8 +328,9 @@ const FwdStage kS5P3[5] = {{kRkAxpy, 0, 1, -1, {B10, 0, 0}},
 // forward steps through the stage store: S[5m + k] is the input of stage k
 // of local step m (S[5m] its start state), T the matching face traces;
 // stage g = 5*step + k reads running-max slot g of hist and writes slot g+1
+// (a rerun writes the values already there); launched on st
 int forward_steps(sddc_ctx *ctx, double dt, int step0, int nsteps, double *const *S, double *const *T, double *hist,
-                  int n1, int n2, double *force, double *cmax)
+                  int n1, int n2, double *force, double *cmax, cudaStream_t st)
 {
     const size_t fgrid = (ctx->ncell + ctx->cpb - 1) / ctx->cpb;
     for (int m = 0; m < nsteps; m++) {
@@ -359,7 +360,7 @@ int forward_steps(sddc_ctx *ctx, double dt, int step0, int nsteps, double *const
                 a.jac = nullptr;
                 a.jac_inv = 0;
             }
-            CKA(launch_stage_exact(ctx->N, ctx->cpb, false, a, ctx->ops, ctx->stream));
+            CKA(launch_stage_exact(ctx->N, ctx->cpb, false, a, ctx->ops, st));
         }
         const int n = step0 + m + 1;
         if (force && n >= n1 && n <= n2) CKA(wall_force(ctx, T[5 * (m + 1)], force + 2 * n));
@@ -459,6 +460,38 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
     if (grad)
         for (auto &a : A)
             if ((rc = rb.get(ctx, &a, nq, "adjoint register"))) return rc;
+    // the reverse sweep recomputes segment s - 1 into a second stage store
+    // (with its own per-CTA maxima) on a second stream while it reverses
+    // segment s from the first
+    const bool overlap = grad && nseg > 1;
+    std::vector<double *> S2(overlap ? 5 * segmax + 1 : 0), T2(overlap ? 5 * segmax + 1 : 0);
+    double *cmax2 = nullptr;
+    if (overlap) {
+        for (int i = 0; i <= 5 * segmax; i++)
+            if ((rc = rb.get(ctx, &S2[i], nq, "stage state")) || (rc = rb.get(ctx, &T2[i], tr, "stage traces"))) return rc;
+        if ((rc = rb.get(ctx, &cmax2, (size_t)5 * segmax * 2 * ((ctx->ncell + ctx->cpb - 1) / ctx->cpb), "CTA maxima")))
+            return rc;
+    }
+
+    // streams and events of the overlapped reverse sweep; on every exit the
+    // streams are drained (before the run buffers go) and the context's
+    // stream is restored
+    struct Overlap {
+        sddc_ctx *ctx = nullptr;
+        cudaStream_t saved = nullptr, rs = nullptr, hs = nullptr;  // recompute stream, reverse stream
+        cudaEvent_t ready[2] = {}, freed[2] = {}, join = nullptr;
+        ~Overlap()
+        {
+            if (rs) cudaStreamSynchronize(rs);
+            if (hs) cudaStreamSynchronize(hs);
+            if (saved) ctx->stream = saved;
+            for (cudaEvent_t e : {ready[0], ready[1], freed[0], freed[1], join})
+                if (e) cudaEventDestroy(e);
+            if (rs) cudaStreamDestroy(rs);
+            if (hs) cudaStreamDestroy(hs);
+        }
+    } ov;
+    ov.ctx = ctx;
 
     cudaEvent_t ev[3];
     for (auto &e : ev) CKA(cudaEventCreate(&e));
@@ -481,7 +514,9 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
         CKA(cudaMemcpyAsync(S[0], ckpt[s], nq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         CKA(launch_trace_exact(ctx->N, ctx->ncell, S[0], T[0], ctx->ops, ctx->stream));
         if (s == 0 && o->n1 == 0) CKA(wall_force(ctx, T[0], force));
-        if ((rc = forward_steps(ctx, o->dt, step0, nst, S.data(), T.data(), hist, o->n1, o->n2, force, cmax))) return rc;
+        if ((rc = forward_steps(ctx, o->dt, step0, nst, S.data(), T.data(), hist, o->n1, o->n2, force, cmax,
+                                ctx->stream)))
+            return rc;
         if (s + 1 < nseg)
             CKA(cudaMemcpyAsync(ckpt[s + 1], S[5 * nst], nq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     }
@@ -517,6 +552,18 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
     float rev_ms = 0.0f;
     if (grad) {
         // ---- reverse sweep ---------------------------------------------------------
+        if (overlap) {
+            int lo = 0, hi = 0;
+            CKA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CKA(cudaStreamCreateWithPriority(&ov.rs, cudaStreamNonBlocking, lo));
+            CKA(cudaStreamCreateWithPriority(&ov.hs, cudaStreamNonBlocking, hi));
+            for (cudaEvent_t *e : {&ov.ready[0], &ov.ready[1], &ov.freed[0], &ov.freed[1], &ov.join})
+                CKA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            // the reverse sweep on the high-priority stream (the forward run
+            // is complete: the stream was synchronised above)
+            ov.saved = ctx->stream;
+            ctx->stream = ov.hs;
+        }
         CKA(cudaMemsetAsync(w->acc, 0, sizeof(AdjScalars), ctx->stream));
         CKA(cudaMemsetAsync(w->rec_n, 0, 4 * sizeof(int), ctx->stream));
         w->at_ready = false;
@@ -538,66 +585,91 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
             r.scale_next = B54 * o->dt;
             if ((rc = reverse_stage(ctx, r))) return rc;
         }
+        // the two stage stores: store cur holds the segment being reversed,
+        // the other one receives the next (earlier) segment on the recompute
+        // stream.  The reverse sweep runs on a stream of the highest priority,
+        // so that the recompute takes only the SMs it leaves idle (the
+        // one-block reductions, the tails of its launches).
+        std::vector<double *> *SS[2] = {&S, &S2}, *TT[2] = {&T, &T2};
+        double *CM[2] = {cmax, cmax2};
+        int cur = 0;
+        auto recompute = [&](int seg, int buf, cudaStream_t st) -> int {
+            const int s0 = seg * K, n = std::min(K, ns - s0);
+            CKA(cudaMemcpyAsync((*SS[buf])[0], ckpt[seg], nq * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CKA(launch_trace_exact(ctx->N, ctx->ncell, (*SS[buf])[0], (*TT[buf])[0], ctx->ops, st));
+            return forward_steps(ctx, o->dt, s0, n, SS[buf]->data(), TT[buf]->data(), hist, 0, -1, nullptr, CM[buf], st);
+        };
         for (int s = nseg - 1; s >= 0; s--) {
             const int step0 = s * K, nst = std::min(K, ns - step0);
-            if (s != nseg - 1) {  // recompute the segment's stage states
-                CKA(cudaMemcpyAsync(S[0], ckpt[s], nq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-                CKA(launch_trace_exact(ctx->N, ctx->ncell, S[0], T[0], ctx->ops, ctx->stream));
-                if ((rc = forward_steps(ctx, o->dt, step0, nst, S.data(), T.data(), hist, 0, -1, nullptr, cmax))) return rc;
+            if (overlap && s > 0) {  // segment s - 1 into the other store, once segment s + 1 has left it
+                if (s < nseg - 1) CKA(cudaStreamWaitEvent(ov.rs, ov.freed[1 - cur], 0));
+                if ((rc = recompute(s - 1, 1 - cur, ov.rs))) return rc;
+                CKA(cudaEventRecord(ov.ready[1 - cur], ov.rs));
             }
+            if (s < nseg - 1) CKA(cudaStreamWaitEvent(ctx->stream, ov.ready[cur], 0));
+            double *const *S_ = SS[cur]->data(), *const *T_ = TT[cur]->data();
+            double *cmax_ = CM[cur];
             for (int m = nst - 1; m >= 0; m--) {
                 const int n = step0 + m, i = 5 * m;
                 const size_t fgrid = (ctx->ncell + ctx->cpb - 1) / ctx->cpb;
                 auto maxima = [&](RevStage &r, int k) {
                     const size_t g = (size_t)5 * n + k;
-                    r.cta_max = cmax + (size_t)(5 * m + k) * 2 * fgrid;
+                    r.cta_max = cmax_ + (size_t)(5 * m + k) * 2 * fgrid;
                     r.L = H[2 * g];
                     r.U = H[2 * g + 1];
                     r.Lnext = H[2 * g + 2];
                     r.Unext = H[2 * g + 3];
                     if (r.Lnext > r.L || r.Unext > r.U) owners++;
                 };
-                RevStage r5;  // stage 5: input Q4 = S[i+4]
-                r5.q = S[i + 4]; r5.t = T[i + 4]; r5.xbar = Ab[5]; r5.scale = B54 * o->dt;
+                RevStage r5;  // stage 5: input Q4 = S_[i+4]
+                r5.q = S_[i + 4]; r5.t = T_[i + 4]; r5.xbar = Ab[5]; r5.scale = B54 * o->dt;
                 r5.ra = Ab[5]; r5.wa = A54; r5.out = Ab[4]; r5.wd = A52; r5.out2 = Ab[2];
-                r5.q_next = S[i + 3]; r5.scale_next = B43 * o->dt;
+                r5.q_next = S_[i + 3]; r5.scale_next = B43 * o->dt;
                 maxima(r5, 4);
                 if ((rc = reverse_stage(ctx, r5))) return rc;
-                RevStage r4;  // stage 4: input Q3 = S[i+3]
-                r4.q = S[i + 3]; r4.t = T[i + 3]; r4.xbar = Ab[4]; r4.scale = B43 * o->dt;
+                RevStage r4;  // stage 4: input Q3 = S_[i+3]
+                r4.q = S_[i + 3]; r4.t = T_[i + 3]; r4.xbar = Ab[4]; r4.scale = B43 * o->dt;
                 r4.ra = Ab[4]; r4.wa = A43; r4.out = Ab[3]; r4.wd = A40; r4.out2 = Ab[0];
-                r4.q_next = S[i + 2]; r4.scale_next = B32 * o->dt;
+                r4.q_next = S_[i + 2]; r4.scale_next = B32 * o->dt;
                 maxima(r4, 3);
                 if ((rc = reverse_stage(ctx, r4))) return rc;
-                RevStage r3;  // stage 3: input Q2 = S[i+2]
-                r3.q = S[i + 2]; r3.t = T[i + 2]; r3.xbar = Ab[3]; r3.scale = B32 * o->dt;
+                RevStage r3;  // stage 3: input Q2 = S_[i+2]
+                r3.q = S_[i + 2]; r3.t = T_[i + 2]; r3.xbar = Ab[3]; r3.scale = B32 * o->dt;
                 r3.ra = Ab[2]; r3.wa = 1.0; r3.rb = Ab[3]; r3.wb = A32; r3.out = Ab[2];
                 r3.rc = Ab[0]; r3.wc = 1.0; r3.wd = A30; r3.out2 = Ab[0];
-                r3.q_next = S[i + 1]; r3.scale_next = B21 * o->dt;
+                r3.q_next = S_[i + 1]; r3.scale_next = B21 * o->dt;
                 maxima(r3, 2);
                 if ((rc = reverse_stage(ctx, r3))) return rc;
-                RevStage r2;  // stage 2: input Q1 = S[i+1]
-                r2.q = S[i + 1]; r2.t = T[i + 1]; r2.xbar = Ab[2]; r2.scale = B21 * o->dt;
+                RevStage r2;  // stage 2: input Q1 = S_[i+1]
+                r2.q = S_[i + 1]; r2.t = T_[i + 1]; r2.xbar = Ab[2]; r2.scale = B21 * o->dt;
                 r2.ra = Ab[2]; r2.wa = 1.0; r2.out = Ab[1];
-                r2.q_next = S[i]; r2.scale_next = B10 * o->dt;
+                r2.q_next = S_[i]; r2.scale_next = B10 * o->dt;
                 maxima(r2, 1);
                 if ((rc = reverse_stage(ctx, r2))) return rc;
-                RevStage r1;  // stage 1: input Q0 = S[i], the state after n steps
-                r1.q = S[i]; r1.t = T[i]; r1.xbar = Ab[1]; r1.scale = B10 * o->dt;
+                RevStage r1;  // stage 1: input Q0 = S_[i], the state after n steps
+                r1.q = S_[i]; r1.t = T_[i]; r1.xbar = Ab[1]; r1.scale = B10 * o->dt;
                 r1.ra = Ab[0]; r1.wa = 1.0; r1.rb = Ab[1]; r1.wb = 1.0; r1.out = Ab[0];
                 const bool in = n >= o->n1 && n <= o->n2;
                 r1.sx = in ? sx : 0.0;
                 r1.sy = in ? sy : 0.0;
                 if (m > 0) {  // stage 5 of step n - 1 (its input is recomputed with the segment)
-                    r1.q_next = S[i - 1];
+                    r1.q_next = S_[i - 1];
                     r1.scale_next = B54 * o->dt;
                 }
                 maxima(r1, 0);
                 if ((rc = reverse_stage(ctx, r1))) return rc;
                 std::swap(Ab[0], Ab[5]);  // the adjoint of the state after n steps
             }
+            if (overlap) CKA(cudaEventRecord(ov.freed[cur], ctx->stream));
+            cur = 1 - cur;
         }
         CKA(cudaEventRecord(ev[2], ctx->stream));
+        if (overlap) {  // back to the context's stream, after the sweep
+            CKA(cudaEventRecord(ov.join, ov.hs));
+            CKA(cudaStreamWaitEvent(ov.saved, ov.join, 0));
+            ctx->stream = ov.saved;
+            ov.saved = nullptr;
+        }
         if (Qbar0) CKA(cudaMemcpyAsync(Qbar0, Ab[5], nq * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CKA(cudaMemcpyAsync(w->host, w->acc, sizeof(AdjScalars), cudaMemcpyDeviceToHost, ctx->stream));
         CKA(cudaStreamSynchronize(ctx->stream));
@@ -627,7 +699,9 @@ extern "C" int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *o, doubl
             const int step0 = (nseg - 1) * K;
             CKA(cudaMemcpyAsync(S[0], ckpt[nseg - 1], nq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
             CKA(launch_trace_exact(ctx->N, ctx->ncell, S[0], T[0], ctx->ops, ctx->stream));
-            if ((rc = forward_steps(ctx, o->dt, step0, last, S.data(), T.data(), hist, 0, -1, nullptr, cmax))) return rc;
+            if ((rc = forward_steps(ctx, o->dt, step0, last, S.data(), T.data(), hist, 0, -1, nullptr, cmax,
+                                    ctx->stream)))
+                return rc;
         }
         CKA(cudaMemcpyAsync(ctx->reg[0], fin, nq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         const double *hl = &H[2 * (size_t)5 * ns];

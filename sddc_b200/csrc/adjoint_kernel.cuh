@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
         for (int r = 0; r < NP; r++) {
             double acc = 0.0;
 #pragma unroll
-            for (int s = 0; s < N; s++) acc = acc + qs[s] * sL[r * N + s];
+            for (int s = 0; s < N; s++) acc = acc + qs[s] * ops.L[r * N + s];
             o[r * 9] = acc;
         }
     }
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
         for (int r = 0; r < NP; r++) {
             double acc = 0.0;
 #pragma unroll
-            for (int i = 0; i < N; i++) acc += sM[r * N + i] * x[i];
+            for (int i = 0; i < N; i++) acc += ops.M[r * N + i] * x[i];
             if (v < 9) {
                 sFb[c * kF + ((f * N + l) * NP + r) * 9 + v] = acc;
             } else {
@@ -829,9 +829,11 @@ __global__ void __launch_bounds__(adj_threads(N, CPB), 4) vjp_kernel(const VjpAr
         const int lane = tid & 31, wid = tid >> 5;
         constexpr int NW = NT / 32;
         double v[7] = {cbar, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5]};
+        // the free-stream adjoints are zero away from boundary faces: a warp
+        // whose lanes all hold zero skips that sum
 #pragma unroll
         for (int m = 0; m < 7; m++) {
-            v[m] = warp_sum(v[m]);
+            if (m == 0 || __any_sync(0xffffffffu, v[m] != 0.0)) v[m] = warp_sum(v[m]);
             if (lane == 0) sRed[m * 32 + wid] = v[m];
         }
         __syncthreads();
