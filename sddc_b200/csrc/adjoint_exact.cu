@@ -9,7 +9,8 @@ namespace sddc {
 
 template <int N> static void locate_n(int nblk, const LocateArgs &a, const Ops &ops, cudaStream_t st)
 {
-    adj_locate_kernel<N><<<nblk, 128, 0, st>>>(a, ops);
+    // one thread per forward CTA checks its recorded maxima
+    adj_locate_kernel<N><<<(nblk + kLocateThreads - 1) / kLocateThreads, kLocateThreads, 0, st>>>(a, ops, nblk);
 }
 
 cudaError_t launch_adj_locate(int N, int nblk, const LocateArgs &a, const Ops &ops, cudaStream_t st)

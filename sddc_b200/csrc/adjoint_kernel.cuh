@@ -874,6 +874,8 @@ static __global__ void __launch_bounds__(kRedThreads) adj_reduce_kernel(int nblk
     __shared__ double ps[6];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    // unrolled so that the loads of several partials are in flight at once
+#pragma unroll 8
     for (int b = tid; b < nblk; b += kRedThreads)
 #pragma unroll
         for (int m = 0; m < 7; m++) v[m] += part[(size_t)m * nblk + b];
@@ -931,11 +933,13 @@ static __global__ void __launch_bounds__(kRedThreads) adj_reduce_kernel(int nblk
 }
 
 // ---- where a running maximum was raised --------------------------------------------
-// One CTA per CTA of the forward stage (cpb cells each).  A CTA whose
-// recorded maximum equals the stage's new running max recomputes, in the
-// exact form (its translation unit is compiled with -fmad=false, like the
-// forward stage kernel), the wave speed and velocity maximum of its points
-// and records the gradient of each one equal to the new maximum.
+// Each thread checks the recorded maxima of one CTA of the forward stage
+// (cpb cells each; a block covers 128 of them).  For every CTA whose
+// recorded maximum equals the stage's new running max, in ascending order,
+// the block recomputes, in the exact form (its translation unit is compiled
+// with -fmad=false, like the forward stage kernel), the wave speed and
+// velocity maximum of its points and records the gradient of each one equal
+// to the new maximum.
 struct LocateArgs {
     int ncell, vismode, cpb;
     double c_h;
@@ -948,15 +952,15 @@ struct LocateArgs {
     RecSink rs;
 };
 
+constexpr int kLocateThreads = 128;
+
+// the points of forward CTA `tile` (cpb cells) that attain the new maximum
 template <int N>
-__global__ void __launch_bounds__(128) adj_locate_kernel(const LocateArgs a, const Ops ops)
+__device__ void locate_tile(const LocateArgs &a, const Ops &ops, int tile, bool e, bool u)
 {
     using ML = MetLayout<N>;
     constexpr int NQ = 9 * N * N, NP = N + 1;
-    const bool e = a.hit_eig && a.cta_max[2 * blockIdx.x] == a.eig_max;
-    const bool u = a.hit_um && a.cta_max[2 * blockIdx.x + 1] == a.um_max;
-    if (!e && !u) return;
-    const int c0 = blockIdx.x * a.cpb, ncl = min(a.cpb, a.ncell - c0);
+    const int c0 = tile * a.cpb, ncl = min(a.cpb, a.ncell - c0);
     // flux-point state of line (fam, line) at point r, as phase A computes it
     auto interp = [&](int cell, int fam, int line, int r, double *qf) {
         const double *qc = a.q + (size_t)cell * NQ;
@@ -1026,6 +1030,31 @@ __global__ void __launch_bounds__(128) adj_locate_kernel(const LocateArgs a, con
             }
         }
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kLocateThreads) adj_locate_kernel(const LocateArgs a, const Ops ops, int ntiles)
+{
+    __shared__ unsigned sE[kLocateThreads / 32], sU[kLocateThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    {
+        const int bt = blockIdx.x * kLocateThreads + threadIdx.x;
+        const bool e = bt < ntiles && a.hit_eig && a.cta_max[2 * bt] == a.eig_max;
+        const bool u = bt < ntiles && a.hit_um && a.cta_max[2 * bt + 1] == a.um_max;
+        const unsigned me = __ballot_sync(0xffffffffu, e), mu = __ballot_sync(0xffffffffu, u);
+        if (lane == 0) {
+            sE[wid] = me;
+            sU[wid] = mu;
+        }
+    }
+    __syncthreads();
+    for (int w = 0; w < kLocateThreads / 32; w++)
+        for (unsigned m = sE[w] | sU[w]; m; m &= m - 1) {
+            const int bit = __ffs(m) - 1;
+            const int tile = blockIdx.x * kLocateThreads + 32 * w + bit;
+            const bool e = (sE[w] >> bit) & 1u, u = (sU[w] >> bit) & 1u;
+            locate_tile<N>(a, ops, tile, e, u);
+        }
 }
 
 // ---- the objective: force on the wall faces -------------------------------------------
