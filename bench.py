@@ -341,7 +341,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(Q0.nbytes), "d2h_bytes_per_step": int(Q0.nbytes) + 32,
                 "steps": e2e_steps, "path": "sddc_set_state + sddc_rk_step + sddc_get_state + sddc_monitor"},
         "gpu_launches": 5 * steps,
-        "ensemble": ensemble_run(torch) if not args.no_ensemble and single else None,
+        "ensemble": ensemble_run(torch, gpu_index) if not args.no_ensemble and single else None,
         "adjoint": adjoint_bench(torch, nsteps=args.adjoint_steps, n1=args.adjoint_steps * 5 // 6,
                                  n2=args.adjoint_steps) if args.adjoint_steps and single else None,
         "output": output_bench(torch, solver_mod, c.mesh, t, ph, Q0, dt, TILES["mixed"]["cells_per_cta"])
@@ -451,7 +451,7 @@ def orszag_tang_run(torch, n=1024, t_end=0.5, chunk=200, max_steps=0, forms=("fp
     return res
 
 
-def ensemble_run(torch, ncase=64, steps=1000, warmup=3, seed=0):
+def ensemble_run(torch, gpu_index=None, ncase=64, steps=1000, warmup=3, seed=0):
     """64 cylinder cases (p = 3, mixed, sizes uniform over 16x32..128x256,
     per-case CFL time steps), 1000 RK3 steps, in one launch per stage: one
     CTA per tile, and persistent (as many CTAs as are resident, each walking
@@ -482,11 +482,16 @@ def ensemble_run(torch, ncase=64, steps=1000, warmup=3, seed=0):
             best, best_t = cpb, tt
         b.close()
     launches = {}
+    clocks = {}
     for mode in ("per_tile", "persistent"):
         b = ensemble.Batch(members, precision="mixed", cells_per_cta=best, persistent=mode == "persistent")
         b.reset()
         b.step(warmup)
-        t = timed(lambda: b.step(steps), b.solver.stream_handle())
+        # the clocks of the batched runs (after the runs before them, a
+        # power cap may hold the SM clock below its maximum)
+        with Clocks(gpu_index if gpu_index is not None else "0") as ck:
+            t = timed(lambda: b.step(steps), b.solver.stream_handle())
+        clocks[mode] = ck.summary()
         q = b.solver.state()["Q"]
         launches[mode] = (t, q, bool(np.isfinite(q).all()))
         b.close()
@@ -524,7 +529,8 @@ def ensemble_run(torch, ncase=64, steps=1000, warmup=3, seed=0):
             "form": "mixed", "cells_per_cta": best, "finite": finite,
             "batched": {"value": units / t_batch, "unit": UNIT, "s_per_step": t_batch / steps,
                         "launch": mode_best},
-            "batched_by_launch": {k: {"value": units / v[0], "unit": UNIT, "s_per_step": v[0] / steps}
+            "batched_by_launch": {k: {"value": units / v[0], "unit": UNIT, "s_per_step": v[0] / steps,
+                                      "clocks": clocks[k]}
                                   for k, v in launches.items()},
             "sequential": {"value": units / t_seq["mixed"], "unit": UNIT, "s_per_step": t_seq["mixed"] / steps},
             "batched_over_sequential": t_seq["mixed"] / t_batch,

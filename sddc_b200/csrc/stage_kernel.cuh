@@ -305,11 +305,17 @@ template <int N, int CPB, typename R, bool DIAG> constexpr size_t stage_smem_byt
 // CTAs per SM the kernel is compiled for: as many as the 228 KB of shared
 // memory per SM hold (1 KB per CTA is the driver's), but no fewer than 96
 // registers per thread (64 for the 6-cell tile: 6 CTAs of 160 threads at
-// N = 5 in the mixed form, measured faster than 5 CTAs with 80 registers)
+// N = 5 in the mixed form, measured faster than 5 CTAs with 80 registers),
+// and at most 8, except for the mixed form's 6-cell tile at N >= 4, which
+// may take what shared memory allows up to the SM's 32 CTAs and 2048
+// threads: 9 CTAs of 96 threads at N = 4 (70 registers; compiled for 8 it
+// took 74, allocated as 80, and held 8; measured 5% faster)
 template <int N, int CPB, typename R, bool DIAG> constexpr int stage_min_blocks()
 {
+    constexpr bool kWide = CPB == 6 && sizeof(R) == sizeof(float) && N >= 4;
+    const int bmax = kWide ? (2048 / stage_threads(N, CPB) < 32 ? 2048 / stage_threads(N, CPB) : 32) : 8;
     int b = (int)((228 * 1024) / (stage_smem_bytes<N, CPB, R, DIAG>() + 1024));
-    b = b < 1 ? 1 : (b > 8 ? 8 : b);
+    b = b < 1 ? 1 : (b > bmax ? bmax : b);
     while (b > 1 && 65536 / (stage_threads(N, CPB) * b) < (CPB == 6 ? 64 : 96)) b--;
     return b;
 }
