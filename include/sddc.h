@@ -331,7 +331,10 @@ typedef struct sddc_adjoint_stats {
    (6) = dJ/d(rinf, pinf, uinf, vinf, bxinf, byinf) through the boundary
    states, the normalisation of C held fixed.  The context ends at the final
    state and maxima, as after sddc_rk_step(ctx, dt, nsteps) in the exact
-   form.  stats is nullable. */
+   form.  The reverse sweep recomputes the next segment on a second stream
+   (two stores of 5*checkpoint_every+1 stage states and traces) while it
+   reverses the current one; both streams are the call's own and drained
+   before it returns.  stats is nullable. */
 int sddc_adjoint_run(sddc_ctx *ctx, const sddc_adjoint_opts *opts, double *obj, double *Qbar0, double *parbar,
                      sddc_adjoint_stats *stats);
 
