@@ -47,8 +47,8 @@ constexpr int kMaxN = 6;
 
 // threads per cell: one per face point (4N); the 6-cell tile gives each
 // solution point its own thread where there are more of those (N*N > 4N, N
-// >= 5), so that the residual phase takes one round (measured the fastest
-// tile of the mixed and exact forms at N = 5, with at most 80 registers)
+// >= 5), so that the residual phase takes one round (the fastest tile of all
+// three forms at N = 5: 64 registers and 6 CTAs per SM in the mixed form)
 __host__ __device__ constexpr int stage_tpc(int n, int cpb) { return cpb == 6 && n * n > 4 * n ? n * n : 4 * n; }
 // threads of a CTA owning cpb cells, rounded up to whole warps
 __host__ __device__ constexpr int stage_threads(int n, int cpb) { return (stage_tpc(n, cpb) * cpb + 31) / 32 * 32; }
